@@ -1,0 +1,271 @@
+"""gpupi_b200: B200-native batched multi-precision arithmetic and Chudnovsky pi.
+
+Python binding of ``libgpupi_b200.so`` (C ABI in ``include/gpupi_c.h``).  The
+functions mirror gpupi's batched API (``batch_arith.h``): every operand is a
+batch of N unsigned integers stored as little-endian 32-bit limbs, item i at
+``data + i*stride`` (stride 0 broadcasts one row).  Device memory is handled
+with torch tensors (int32 storage reinterpreted as uint32 limbs); all
+arithmetic runs in this library's CUDA kernels.
+
+There is no CPU fallback: importing works without a GPU (for build checks),
+but every compute call raises if the native library or a CUDA device is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libgpupi_b200.so"
+CLI_PATH = _HERE / "pi_bs_gpu"
+
+_lib = None
+
+_u32 = ctypes.c_uint32
+_p = ctypes.c_void_p
+_i32 = ctypes.c_int32
+
+# (name, restype, argtypes) for every C ABI symbol in include/gpupi_c.h
+_SIGS = [
+    ("gpupi_version", ctypes.c_char_p, []),
+    ("gpupi_launch_count", ctypes.c_uint64, []),
+    ("gpupi_set_stream", ctypes.c_int, [_p]),
+    ("gpupi_device_sync", ctypes.c_int, []),
+    ("gpupi_ctx_create", _p, []),
+    ("gpupi_ctx_destroy", None, [_p]),
+    ("gpupi_ctx_workspace_size", ctypes.c_size_t, [_p]),
+    ("gpupi_ctx_ensure_workspace", ctypes.c_int, [_p, ctypes.c_size_t]),
+    ("gpupi_mp_mul", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_add", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_sub", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_shift_add", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_shift_sub", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_add_small", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_sub_small", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_mul_small", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_mp_exactdiv_small", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _u32]),
+    ("gpupi_mp_shift_bits", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _i32]),
+    ("gpupi_mp_bitlength_max", ctypes.c_int, [_p, _u32, _p, _u32, _u32, ctypes.POINTER(_u32)]),
+    ("gpupi_mp_limblength_max", ctypes.c_int, [_p, _u32, _p, _u32, _u32, ctypes.POINTER(_u32)]),
+    ("gpupi_mul_naive", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
+    ("gpupi_mul_ntt", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
+    ("gpupi_decimal_naive", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32]),
+    ("gpupi_convert_decimal", ctypes.c_int, [_p, _p, _u32, _u32, _u32, _u32, _p]),
+    ("gpupi_pi_compute", ctypes.c_int,
+     [_p, _u32, _u32, _p, ctypes.c_size_t, _p, ctypes.c_size_t, ctypes.POINTER(_u32)]),
+    ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
+]
+
+C_ABI_SYMBOLS = [s[0] for s in _SIGS]
+
+
+class GpupiError(RuntimeError):
+    pass
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise GpupiError(f"{LIB_PATH} is missing: run gpupi_b200/build.py (or __graft_entry__.build())")
+        l = ctypes.CDLL(str(LIB_PATH))
+        for name, res, args in _SIGS:
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise GpupiError(f"{what} failed with cudaError {rc}")
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise GpupiError("gpupi_b200 needs a CUDA device; there is no CPU fallback")
+    return torch
+
+
+# ---------------------------------------------------------------------------
+# Device buffers
+# ---------------------------------------------------------------------------
+class DeviceLimbs:
+    """A device buffer of uint32 limbs (torch int32 storage)."""
+
+    def __init__(self, words: int):
+        torch = _torch()
+        self.t = torch.zeros(max(int(words), 1), dtype=torch.int32, device="cuda")
+        self.words = int(words)
+
+    @classmethod
+    def from_numpy(cls, a: np.ndarray) -> "DeviceLimbs":
+        torch = _torch()
+        a = np.ascontiguousarray(a, dtype=np.uint32).reshape(-1)
+        d = cls(a.size)
+        if a.size:
+            d.t[: a.size].copy_(torch.from_numpy(a.view(np.int32)))
+        return d
+
+    @property
+    def ptr(self) -> int:
+        return self.t.data_ptr()
+
+    def at(self, offset_words: int) -> int:
+        return self.ptr + 4 * int(offset_words)
+
+    def numpy(self) -> np.ndarray:
+        _torch().cuda.synchronize()
+        return self.t[: self.words].cpu().numpy().view(np.uint32)
+
+
+class DeviceBytes:
+    def __init__(self, n: int):
+        torch = _torch()
+        self.t = torch.zeros(max(int(n), 1), dtype=torch.uint8, device="cuda")
+        self.n = int(n)
+
+    @property
+    def ptr(self) -> int:
+        return self.t.data_ptr()
+
+    def text(self) -> str:
+        _torch().cuda.synchronize()
+        return bytes(self.t[: self.n].cpu().numpy()).decode("ascii")
+
+
+# ---------------------------------------------------------------------------
+# Context and batched ops (gpupi batch_arith.h)
+# ---------------------------------------------------------------------------
+class Context:
+    """Wraps BatchMPContext (NTT tables + grow-only workspace)."""
+
+    def __init__(self):
+        _torch()
+        self.h = lib().gpupi_ctx_create()
+        if not self.h:
+            raise GpupiError("gpupi_ctx_create failed")
+
+    def close(self) -> None:
+        if self.h:
+            lib().gpupi_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def workspace_size(self) -> int:
+        return lib().gpupi_ctx_workspace_size(self.h)
+
+    # Each op takes raw device addresses (ints), lengths and strides.
+    def mul(self, N, A, La, sA, B, Lb, sB, C, Lc, sC):
+        _check(lib().gpupi_mp_mul(self.h, N, A, La, sA, B, Lb, sB, C, Lc, sC), "batch_mp_mul")
+
+    def add(self, N, A, La, sA, B, Lb, sB, C, Lc, sC):
+        _check(lib().gpupi_mp_add(self.h, N, A, La, sA, B, Lb, sB, C, Lc, sC), "batch_mp_add")
+
+    def sub(self, N, A, La, sA, B, Lb, sB, C, Lc, sC):
+        _check(lib().gpupi_mp_sub(self.h, N, A, La, sA, B, Lb, sB, C, Lc, sC), "batch_mp_sub")
+
+    def shift_add(self, N, A, La, sA, B, Lb, sB, shift, C, Lc, sC):
+        _check(lib().gpupi_mp_shift_add(self.h, N, A, La, sA, B, Lb, sB, shift, C, Lc, sC), "batch_mp_shift_add")
+
+    def shift_sub(self, N, A, La, sA, B, Lb, sB, shift, C, Lc, sC):
+        _check(lib().gpupi_mp_shift_sub(self.h, N, A, La, sA, B, Lb, sB, shift, C, Lc, sC), "batch_mp_shift_sub")
+
+    def add_small(self, N, A, La, sA, b, C, Lc, sC):
+        _check(lib().gpupi_mp_add_small(self.h, N, A, La, sA, b, C, Lc, sC), "batch_mp_add_small")
+
+    def sub_small(self, N, A, La, sA, b, C, Lc, sC):
+        _check(lib().gpupi_mp_sub_small(self.h, N, A, La, sA, b, C, Lc, sC), "batch_mp_sub_small")
+
+    def mul_small(self, N, A, La, sA, b, C, Lc, sC):
+        _check(lib().gpupi_mp_mul_small(self.h, N, A, La, sA, b, C, Lc, sC), "batch_mp_mul_small")
+
+    def exactdiv_small(self, N, A, La, sA, b):
+        _check(lib().gpupi_mp_exactdiv_small(self.h, N, A, La, sA, b), "batch_mp_exactdiv_small")
+
+    def shift_bits(self, N, A, La, sA, B, Lb, sB, shift):
+        _check(lib().gpupi_mp_shift_bits(self.h, N, A, La, sA, B, Lb, sB, shift), "batch_mp_shift_bits")
+
+    def bitlength_max(self, N, A, La, sA) -> int:
+        r = _u32(0)
+        _check(lib().gpupi_mp_bitlength_max(self.h, N, A, La, sA, ctypes.byref(r)), "batch_mp_bitlength_max")
+        return r.value
+
+    def limblength_max(self, N, A, La, sA) -> int:
+        r = _u32(0)
+        _check(lib().gpupi_mp_limblength_max(self.h, N, A, La, sA, ctypes.byref(r)), "batch_mp_limblength_max")
+        return r.value
+
+    def mul_ntt(self, N, A, La, sA, B, Lb, sB, C, sC):
+        _check(lib().gpupi_mul_ntt(self.h, N, A, La, sA, B, Lb, sB, C, sC), "batch_mul_ntt")
+
+    def convert_decimal(self, X, Lx, input_bits, total_digits, leaf_digits, out):
+        _check(lib().gpupi_convert_decimal(self.h, X, Lx, input_bits, total_digits, leaf_digits, out),
+               "convert_decimal")
+
+
+def mul_naive(N, A, La, sA, B, Lb, sB, C, sC):
+    _torch()
+    _check(lib().gpupi_mul_naive(N, A, La, sA, B, Lb, sB, C, sC), "batch_mul_naive")
+
+
+def decimal_naive(N, A, L_limb, sA, out, L_dec, s_out):
+    _torch()
+    _check(lib().gpupi_decimal_naive(N, A, L_limb, sA, out, L_dec, s_out), "batch_decimal_naive")
+
+
+def launch_count() -> int:
+    return int(lib().gpupi_launch_count())
+
+
+def set_mul_crossover(v: int) -> None:
+    _check(lib().gpupi_set_mul_crossover(v), "gpupi_set_mul_crossover")
+
+
+# ---------------------------------------------------------------------------
+# Whole pipeline
+# ---------------------------------------------------------------------------
+class PiResult:
+    def __init__(self, digits, convert_digits, ret_len, elapsed_ms, workspace_mb, ret, dec, leaf_digits):
+        self.digits = digits
+        self.convert_digits = convert_digits
+        self.ret_len = ret_len
+        self.elapsed_ms = elapsed_ms
+        self.workspace_mb = workspace_mb
+        self.ret = ret
+        self.dec = dec
+        self.leaf_digits = leaf_digits
+
+
+def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None = None,
+               ret_capacity: int | None = None) -> PiResult:
+    """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional)."""
+    _torch()
+    l = lib()
+    if copy_digits is None:
+        copy_digits = digits
+    if ret_capacity is None:
+        ret_capacity = (int(digits * 3.322) + 31) // 32 + 8
+    ret = np.zeros(max(ret_capacity, 1), dtype=np.uint32)
+    dec = ctypes.create_string_buffer(max(copy_digits, 1))
+    info = (_u32 * 8)()
+    rc = l.gpupi_pi_compute(ctx.h if ctx else None, digits, 0, ret.ctypes.data, ret.size,
+                            ctypes.addressof(dec) if copy_digits else None, copy_digits, info)
+    _check(rc, "gpupi_pi_compute")
+    ret_len = info[1]
+    elapsed = np.frombuffer(np.uint32(info[2]).tobytes(), dtype=np.float32)[0]
+    return PiResult(digits, info[0], ret_len, float(elapsed), info[3], ret[:ret_len].copy(),
+                    dec.raw[:copy_digits].decode("ascii"), info[5])

@@ -1,0 +1,291 @@
+// Batched-MP API: context, array views, validation and multiply dispatch
+// (gpupi batch_arith.cu:1-424, header batch_arith.h:8-152).
+//
+// Same contract as the reference: views are validated (cudaErrorInvalidValue
+// on malformed metadata), scratch comes from one grow-only context
+// workspace, and every op is issued on the library's current stream.  The
+// multiply picks schoolbook below a crossover and the three-prime NTT above it.
+#include "common.cuh"
+#include "batch_add.h"
+#include "batch_add_small.h"
+#include "batch_arith.h"
+#include "batch_bitlength.h"
+#include "batch_exactdiv_small.h"
+#include "batch_mul_naive.h"
+#include "batch_mul_ntt.h"
+#include "batch_mul_small.h"
+#include "batch_shift.h"
+#include "batch_shift_add.h"
+#include "batch_shift_sub.h"
+#include "batch_sub.h"
+#include "batch_sub_small.h"
+
+#include <atomic>
+#include <new>
+
+namespace gpupi {
+
+static cudaStream_t g_stream = 0;
+static std::atomic<uint64_t> g_launches{0};
+
+cudaStream_t current_stream() { return g_stream; }
+void set_current_stream(cudaStream_t s) { g_stream = s; }
+uint64_t launch_counter() { return g_launches.load(); }
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La,
+                uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC);
+bool school_thread_fits(uint32_t La, uint32_t Lb);
+
+// Largest L_a + L_b handled by schoolbook (the reference's crossover is 1024,
+// batch_arith.cu:181).  Overridable for tuning with gpupi_set_mul_crossover().
+static uint32_t g_school_max = 1024u;
+
+}  // namespace gpupi
+
+struct BatchMPContext {
+    NTTPrecomputedTables ntt_tables;
+    uint32_t *workspace;
+    size_t workspace_size_bytes;
+};
+
+namespace {
+
+cudaError_t allocate_tables(BatchMPContext *ctx) {
+    cudaError_t err = cudaMalloc(&ctx->ntt_tables.roots_table_lv1, 65536 * sizeof(uint3));
+    if (err != cudaSuccess) return err;
+    err = cudaMalloc(&ctx->ntt_tables.roots_table_lv2, 65536 * sizeof(uint3));
+    if (err != cudaSuccess) return err;
+    err = cudaMalloc(&ctx->ntt_tables.inv2n_table, 33 * sizeof(uint3));
+    if (err != cudaSuccess) return err;
+    init_ntt_precomputed_tables(&ctx->ntt_tables);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    return cudaDeviceSynchronize();
+}
+
+cudaError_t ensure_workspace(BatchMPContext *ctx, size_t bytes) {
+    if (bytes <= ctx->workspace_size_bytes) return cudaSuccess;
+    uint32_t *p = nullptr;
+    // the old buffer may still be in use by queued work
+    cudaError_t err = cudaStreamSynchronize(gpupi::current_stream());
+    if (err != cudaSuccess) return err;
+    err = cudaMalloc(&p, bytes);
+    if (err != cudaSuccess) return err;
+    if (ctx->workspace) cudaFree(ctx->workspace);
+    ctx->workspace = p;
+    ctx->workspace_size_bytes = bytes;
+    return cudaSuccess;
+}
+
+void release_context(BatchMPContext *ctx) {
+    if (ctx->workspace) cudaFree(ctx->workspace);
+    ctx->workspace = nullptr;
+    ctx->workspace_size_bytes = 0;
+    if (ctx->ntt_tables.roots_table_lv1) cudaFree(ctx->ntt_tables.roots_table_lv1);
+    if (ctx->ntt_tables.roots_table_lv2) cudaFree(ctx->ntt_tables.roots_table_lv2);
+    if (ctx->ntt_tables.inv2n_table) cudaFree(ctx->ntt_tables.inv2n_table);
+    ctx->ntt_tables = NTTPrecomputedTables{};
+}
+
+// batch_arith.cu:89-104
+bool valid_array(const BatchMPArray &a) {
+    if (a.batch_size == 0u) return a.length <= a.stride;
+    if (a.data == nullptr) return false;
+    if (a.stride == 0u) return true;
+    return a.length <= a.stride;
+}
+
+bool same_batch(const BatchMPArray &a, const BatchMPArray &b) { return a.batch_size == b.batch_size; }
+
+}  // namespace
+
+BatchMPArray batch_mp_array_create(uint32_t batch_size, uint32_t length, uint32_t stride) {
+    BatchMPArray a{};
+    a.length = length;
+    a.batch_size = batch_size;
+    a.stride = (stride == 0u) ? length : stride;
+    if (a.length > a.stride) return BatchMPArray{};
+    const size_t bytes = (size_t)a.batch_size * a.stride * sizeof(uint32_t);
+    if (bytes == 0u) return a;
+    if (cudaMalloc(&a.data, bytes) != cudaSuccess) a = BatchMPArray{};
+    return a;
+}
+
+void batch_mp_array_release(BatchMPArray array) {
+    if (array.data) cudaFree(array.data);
+}
+
+BatchMPContext *batch_mp_init() {
+    BatchMPContext *ctx = new (std::nothrow) BatchMPContext{};
+    if (!ctx) return nullptr;
+    if (allocate_tables(ctx) != cudaSuccess) {
+        release_context(ctx);
+        delete ctx;
+        return nullptr;
+    }
+    return ctx;
+}
+
+void batch_mp_destroy(BatchMPContext *ctx) {
+    if (!ctx) return;
+    release_context(ctx);
+    delete ctx;
+}
+
+size_t batch_mp_workspace_size(const BatchMPContext *ctx) { return ctx ? ctx->workspace_size_bytes : 0u; }
+
+cudaError_t batch_mp_ensure_workspace(BatchMPContext *ctx, size_t required_bytes) {
+    if (!ctx) return cudaErrorInvalidValue;
+    return ensure_workspace(ctx, required_bytes);
+}
+
+cudaError_t batch_mp_mul(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
+    if ((uint64_t)C.length != (uint64_t)A.length + B.length) return cudaErrorInvalidValue;
+    if (A.batch_size == 0u || C.length == 0u) return cudaSuccess;
+    const uint32_t L = A.length + B.length;
+    const bool school = A.length == 0u || B.length == 0u ||
+                        gpupi::school_thread_fits(A.length, B.length) ||
+                        (L <= gpupi::g_school_max && L <= (uint32_t)BATCH_MUL_NAIVE_L_MAX);
+    if (school) {
+        gpupi::school_mul(A.data, B.data, C.data, A.batch_size, A.length, B.length, A.stride, B.stride,
+                          C.stride);
+        return cudaGetLastError();
+    }
+    cudaError_t err = ensure_workspace(ctx, batch_mul_ntt_workspace_size(A.batch_size, A.length, B.length));
+    if (err != cudaSuccess) return err;
+    batch_mul_ntt(A.data, B.data, C.data, ctx->workspace, ctx->ntt_tables, A.batch_size, A.length,
+                  B.length, A.stride, B.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_mul_small(BatchMPContext *ctx, BatchMPArray A, uint32_t B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, C)) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(ctx, batch_mul_small_workspace_size(A.batch_size, A.length, C.length));
+    if (err != cudaSuccess) return err;
+    batch_mul_small(A.data, B, C.data, ctx->workspace, A.batch_size, A.length, C.length, A.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_exactdiv_small(BatchMPContext *ctx, BatchMPArray A, uint32_t B) {
+    if (!ctx || !valid_array(A)) return cudaErrorInvalidValue;
+    if (B == 0u || (B & 1u) == 0u || A.length > 128u) return cudaErrorInvalidValue;
+    batch_exactdiv_small(A.data, B, A.batch_size, A.length, A.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_add(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(
+        ctx, batch_add_simple_workspace_size(A.batch_size, A.length, B.length, C.length));
+    if (err != cudaSuccess) return err;
+    batch_add_simple(A.data, B.data, C.data, ctx->workspace, A.batch_size, A.length, B.length, C.length,
+                     A.stride, B.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_add_small(BatchMPContext *ctx, BatchMPArray A, uint32_t B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, C)) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(ctx, batch_add_small_workspace_size(A.batch_size, A.length, C.length));
+    if (err != cudaSuccess) return err;
+    batch_add_small(A.data, B, C.data, ctx->workspace, A.batch_size, A.length, C.length, A.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_shift_add(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, uint32_t shift,
+                               BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
+    if (C.data == A.data || C.data == B.data) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(
+        ctx, batch_shift_add_simple_workspace_size(A.batch_size, A.length, B.length, C.length, shift));
+    if (err != cudaSuccess) return err;
+    batch_shift_add_simple(A.data, B.data, C.data, ctx->workspace, shift, A.batch_size, A.length, B.length,
+                           C.length, A.stride, B.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_shift_sub(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, uint32_t shift,
+                               BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
+    if (C.data == A.data || C.data == B.data) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(
+        ctx, batch_shift_sub_simple_workspace_size(A.batch_size, A.length, B.length, C.length, shift));
+    if (err != cudaSuccess) return err;
+    batch_shift_sub_simple(A.data, B.data, C.data, ctx->workspace, shift, A.batch_size, A.length, B.length,
+                           C.length, A.stride, B.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_sub(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(
+        ctx, batch_sub_simple_workspace_size(A.batch_size, A.length, B.length, C.length));
+    if (err != cudaSuccess) return err;
+    batch_sub_simple(A.data, B.data, C.data, ctx->workspace, A.batch_size, A.length, B.length, C.length,
+                     A.stride, B.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_sub_small(BatchMPContext *ctx, BatchMPArray A, uint32_t B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, C)) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(ctx, batch_sub_small_workspace_size(A.batch_size, A.length, C.length));
+    if (err != cudaSuccess) return err;
+    batch_sub_small(A.data, B, C.data, ctx->workspace, A.batch_size, A.length, C.length, A.stride, C.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_shift_bits(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, int32_t shift_bits) {
+    if (!ctx || !valid_array(A) || !valid_array(B)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B)) return cudaErrorInvalidValue;
+    batch_shift_bits(A.data, B.data, A.batch_size, A.length, B.length, A.stride, B.stride, shift_bits);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_bitlength_max(BatchMPContext *ctx, BatchMPArray A, uint32_t *result) {
+    if (!ctx || !valid_array(A) || !result) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(ctx, batch_bitlength_workspace_size(A.batch_size, A.length));
+    if (err != cudaSuccess) return err;
+    *result = batch_bitlength_max(A.data, ctx->workspace, A.batch_size, A.length, A.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_mp_limblength_max(BatchMPContext *ctx, BatchMPArray A, uint32_t *result) {
+    if (!ctx || !valid_array(A) || !result) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(ctx, batch_bitlength_workspace_size(A.batch_size, A.length));
+    if (err != cudaSuccess) return err;
+    *result = batch_limblength_max(A.data, ctx->workspace, A.batch_size, A.length, A.stride);
+    return cudaGetLastError();
+}
+
+cudaError_t BatchMPArray::compact(BatchMPContext *ctx) {
+    uint32_t len = 0u;
+    cudaError_t err = batch_mp_limblength_max(ctx, *this, &len);
+    if (err != cudaSuccess) return err;
+    length = len;
+    return cudaSuccess;
+}
+
+namespace gpupi {
+// NTT product regardless of the crossover (testing and tuning entry point).
+cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+    if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
+    if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
+    if ((uint64_t)C.length != (uint64_t)A.length + B.length) return cudaErrorInvalidValue;
+    cudaError_t err = ensure_workspace(ctx, batch_mul_ntt_workspace_size(A.batch_size, A.length, B.length));
+    if (err != cudaSuccess) return err;
+    batch_mul_ntt(A.data, B.data, C.data, ctx->workspace, ctx->ntt_tables, A.batch_size, A.length, B.length,
+                  A.stride, B.stride, C.stride);
+    return cudaGetLastError();
+}
+void set_school_max(uint32_t v) { g_school_max = v; }
+uint32_t school_max() { return g_school_max; }
+}  // namespace gpupi

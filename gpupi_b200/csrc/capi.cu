@@ -1,0 +1,193 @@
+// extern "C" boundary of libgpupi_b200.so (declared in include/gpupi_c.h).
+// Thin adapters from plain pointers/sizes to the BatchMPArray API.
+#include "common.cuh"
+#include "batch_arith.h"
+#include "batch_decimal_naive.h"
+#include "batch_mul_naive.h"
+#include "batch_mul_ntt.h"
+#include "convert_decimal.h"
+#include "gpupi_c.h"
+#include "pi_engine.h"
+
+#include <string.h>
+
+struct gpupi_ctx {
+    BatchMPContext *ctx;
+};
+
+namespace {
+inline BatchMPArray view(const uint32_t *d, uint32_t len, uint32_t n, uint32_t stride) {
+    return BatchMPArray{const_cast<uint32_t *>(d), len, n, stride};
+}
+inline BatchMPContext *raw(gpupi_ctx *c) { return c ? c->ctx : nullptr; }
+}  // namespace
+
+extern "C" {
+
+const char *gpupi_version(void) { return "gpupi_b200 0.1 (sm_100a, three-prime NTT)"; }
+
+uint64_t gpupi_launch_count(void) { return gpupi::launch_counter(); }
+
+int gpupi_set_stream(void *s) {
+    gpupi::set_current_stream((cudaStream_t)s);
+    return 0;
+}
+
+int gpupi_device_sync(void) { return (int)cudaDeviceSynchronize(); }
+
+gpupi_ctx *gpupi_ctx_create(void) {
+    BatchMPContext *c = batch_mp_init();
+    if (!c) return nullptr;
+    gpupi_ctx *h = new gpupi_ctx{c};
+    return h;
+}
+
+void gpupi_ctx_destroy(gpupi_ctx *ctx) {
+    if (!ctx) return;
+    batch_mp_destroy(ctx->ctx);
+    delete ctx;
+}
+
+size_t gpupi_ctx_workspace_size(const gpupi_ctx *ctx) { return ctx ? batch_mp_workspace_size(ctx->ctx) : 0; }
+
+int gpupi_ctx_ensure_workspace(gpupi_ctx *ctx, size_t bytes) {
+    return (int)batch_mp_ensure_workspace(raw(ctx), bytes);
+}
+
+int gpupi_mp_mul(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,
+                 uint32_t Lb, uint32_t sB, uint32_t *C, uint32_t Lc, uint32_t sC) {
+    return (int)batch_mp_mul(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), view(C, Lc, N, sC));
+}
+
+int gpupi_mp_add(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,
+                 uint32_t Lb, uint32_t sB, uint32_t *C, uint32_t Lc, uint32_t sC) {
+    return (int)batch_mp_add(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), view(C, Lc, N, sC));
+}
+
+int gpupi_mp_sub(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,
+                 uint32_t Lb, uint32_t sB, uint32_t *C, uint32_t Lc, uint32_t sC) {
+    return (int)batch_mp_sub(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), view(C, Lc, N, sC));
+}
+
+int gpupi_mp_shift_add(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA,
+                       const uint32_t *B, uint32_t Lb, uint32_t sB, uint32_t shift, uint32_t *C, uint32_t Lc,
+                       uint32_t sC) {
+    return (int)batch_mp_shift_add(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), shift, view(C, Lc, N, sC));
+}
+
+int gpupi_mp_shift_sub(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA,
+                       const uint32_t *B, uint32_t Lb, uint32_t sB, uint32_t shift, uint32_t *C, uint32_t Lc,
+                       uint32_t sC) {
+    return (int)batch_mp_shift_sub(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), shift, view(C, Lc, N, sC));
+}
+
+int gpupi_mp_add_small(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, uint32_t b,
+                       uint32_t *C, uint32_t Lc, uint32_t sC) {
+    return (int)batch_mp_add_small(raw(ctx), view(A, La, N, sA), b, view(C, Lc, N, sC));
+}
+
+int gpupi_mp_sub_small(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, uint32_t b,
+                       uint32_t *C, uint32_t Lc, uint32_t sC) {
+    return (int)batch_mp_sub_small(raw(ctx), view(A, La, N, sA), b, view(C, Lc, N, sC));
+}
+
+int gpupi_mp_mul_small(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, uint32_t b,
+                       uint32_t *C, uint32_t Lc, uint32_t sC) {
+    return (int)batch_mp_mul_small(raw(ctx), view(A, La, N, sA), b, view(C, Lc, N, sC));
+}
+
+int gpupi_mp_exactdiv_small(gpupi_ctx *ctx, uint32_t N, uint32_t *A, uint32_t La, uint32_t sA, uint32_t b) {
+    return (int)batch_mp_exactdiv_small(raw(ctx), view(A, La, N, sA), b);
+}
+
+int gpupi_mp_shift_bits(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, uint32_t *B,
+                        uint32_t Lb, uint32_t sB, int32_t shift_bits) {
+    return (int)batch_mp_shift_bits(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), shift_bits);
+}
+
+int gpupi_mp_bitlength_max(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA,
+                           uint32_t *h_result) {
+    return (int)batch_mp_bitlength_max(raw(ctx), view(A, La, N, sA), h_result);
+}
+
+int gpupi_mp_limblength_max(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA,
+                            uint32_t *h_result) {
+    return (int)batch_mp_limblength_max(raw(ctx), view(A, La, N, sA), h_result);
+}
+
+int gpupi_mul_naive(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B, uint32_t Lb,
+                    uint32_t sB, uint32_t *C, uint32_t sC) {
+    if ((uint64_t)La + Lb > (uint64_t)BATCH_MUL_NAIVE_L_MAX) return (int)cudaErrorInvalidValue;
+    batch_mul_naive(const_cast<uint32_t *>(A), const_cast<uint32_t *>(B), C, (int)N, (int)La, (int)Lb, (int)sA,
+                    (int)sB, (int)sC);
+    return (int)cudaGetLastError();
+}
+
+int gpupi_mul_ntt(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,
+                  uint32_t Lb, uint32_t sB, uint32_t *C, uint32_t sC) {
+    return (int)gpupi::mul_ntt_direct(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB),
+                                      view(C, La + Lb, N, sC));
+}
+
+int gpupi_decimal_naive(uint32_t N, const uint32_t *A, uint32_t L_limb, uint32_t sA, char *out, uint32_t L_dec,
+                        uint32_t sO) {
+    if (L_limb > (uint32_t)BATCH_DECIMAL_NAIVE_L_LIMB_MAX) return (int)cudaErrorInvalidValue;
+    batch_decimal_naive(A, out, N, (int)L_limb, sA, (int)L_dec, sO);
+    return (int)cudaGetLastError();
+}
+
+int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *X, uint32_t Lx, uint32_t input_bits,
+                          uint32_t total_digits, uint32_t leaf_digits, char *out) {
+    BatchMPContext *c = raw(ctx);
+    if (!c || leaf_digits == 0u || total_digits % leaf_digits) return (int)cudaErrorInvalidValue;
+    uint32_t ratio = total_digits / leaf_digits, levels = 0u;
+    while (ratio > 1u && (ratio & 1u) == 0u) {
+        ratio >>= 1;
+        ++levels;
+    }
+    if (ratio != 1u) return (int)cudaErrorInvalidValue;
+    ConvertDecimalPowerTable t{};
+    cudaError_t err = convert_decimal_precompute_powers(c, &t, leaf_digits, levels);
+    if (err == cudaSuccess)
+        err = convert_decimal_equal_split(c, view(X, Lx, 1, Lx), input_bits, total_digits, leaf_digits, &t, out);
+    convert_decimal_release_powers(&t);
+    return (int)err;
+}
+
+int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
+                     char *h_digits, size_t digits_cap, uint32_t *info) {
+    gpupi::PiRequest req;
+    req.digits = digits;
+    req.profile_stages = (flags & 1u) != 0u;
+    req.copy_digits = h_digits ? (uint32_t)std::min<size_t>(digits_cap, digits) : 0u;
+    req.ctx = raw(ctx);
+    gpupi::PiOutput out;
+    cudaError_t err = gpupi::pi_run(req, out);
+    if (err != cudaSuccess) return (int)err;
+    if (h_ret) {
+        const size_t n = std::min<size_t>(ret_cap, out.ret.size());
+        memcpy(h_ret, out.ret.data(), n * 4);
+    }
+    if (h_digits && !out.digits.empty()) memcpy(h_digits, out.digits.data(), out.digits.size());
+    if (info) {
+        uint32_t leaf = 0u;
+        gpupi::round_up_decimal_digits(digits, &leaf);
+        info[0] = out.convert_digits;
+        info[1] = out.ret_len;
+        memcpy(&info[2], &out.elapsed_ms, 4);
+        info[3] = (uint32_t)(out.workspace_bytes >> 20);
+        info[4] = (uint32_t)out.stages.size();
+        info[5] = leaf;
+        info[6] = 0u;
+        info[7] = 0u;
+    }
+    return 0;
+}
+
+int gpupi_set_mul_crossover(uint32_t v) {
+    if (v > (uint32_t)BATCH_MUL_NAIVE_L_MAX) return (int)cudaErrorInvalidValue;
+    gpupi::set_school_max(v);
+    return 0;
+}
+
+}  // extern "C"

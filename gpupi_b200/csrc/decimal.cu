@@ -1,0 +1,378 @@
+// Binary -> decimal conversion (gpupi convert_decimal.cu, batch_decimal_naive.cu).
+//
+// Leaf (batch_decimal_naive.cu:16-217): a fraction X / 2^(32L) yields its
+// truncated decimal digits 9 at a time: X *= 10^9, the limb that overflows
+// the top is the next 9-digit chunk.  Here a row is first placed at the top of
+// a fixed-size register array (MAXL limbs, zeros below), so every index is a
+// compile-time constant; one thread converts one row.  Rows longer than 64
+// limbs use one warp per row, where each x10^9 round is a binary-carry add of
+// lo(a_j*10^9) and hi(a_(j-1)*10^9) resolved with ballots.
+//
+// Divide and conquer (convert_decimal.cu:198-474), per level on every row:
+//   high child = top child_bits of X
+//   low child  = top child_bits of (X mod 2^(B-d)) * 5^d      (d = child digits)
+// with 5^d broadcast to all rows (stride 0) so its transform is computed once.
+// The reference's digit semantics (truncating fixed-point splits, 34 margin
+// bits) are reproduced exactly; output is natural order.
+#include "common.cuh"
+#include "batch_arith.h"
+#include "batch_decimal_naive.h"
+#include "batch_shift.h"
+#include "convert_decimal.h"
+
+#include <math.h>
+#include <new>
+#include <vector>
+
+namespace gpupi {
+
+constexpr uint32_t kTen9 = 1000000000u;
+
+// out(pos) for the digit of place 10^-k (k = 1..L_dec):
+//   LSD-first layout (API): pos = L_dec - k;  natural layout: pos = k - 1.
+template <int MAXL, bool NATURAL>
+__global__ void __launch_bounds__(128) k_decimal_thread(const uint32_t *__restrict__ A,
+                                                        char *__restrict__ B, uint32_t N,
+                                                        uint32_t L, uint64_t sA, uint32_t L_dec,
+                                                        uint64_t sB) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < N;
+         row += gridDim.x * blockDim.x) {
+        uint32_t x[MAXL];
+        const uint32_t *ar = A + row * sA;
+        const uint32_t pad = MAXL - L;
+#pragma unroll
+        for (int i = 0; i < MAXL; ++i) x[i] = ((uint32_t)i >= pad) ? ar[i - pad] : 0u;
+        char *out = B + row * sB;
+        for (uint32_t start = 0; start < L_dec; start += 9u) {
+            uint32_t carry = 0u;
+#pragma unroll
+            for (int i = 0; i < MAXL; ++i) {
+                const uint64_t t = (uint64_t)x[i] * kTen9 + carry;
+                x[i] = (uint32_t)t;
+                carry = (uint32_t)(t >> 32);
+            }
+            // carry = next 9 digits (places start+1 .. start+9)
+            const uint32_t cnt = min(9u, L_dec - start);
+            uint32_t v = carry;
+            for (uint32_t m = 9; m > cnt; --m) v /= 10u;   // drop places beyond L_dec
+            for (uint32_t m = cnt; m >= 1; --m) {
+                const uint32_t k = start + m;   // place 10^-k
+                const char d = (char)('0' + v % 10u);
+                v /= 10u;
+                out[NATURAL ? (k - 1u) : (L_dec - k)] = d;
+            }
+        }
+    }
+}
+
+// Warp per row, L <= 32*G limbs.
+template <int G, bool NATURAL>
+__global__ void __launch_bounds__(128) k_decimal_warp(const uint32_t *__restrict__ A,
+                                                      char *__restrict__ B, uint32_t N, uint32_t L,
+                                                      uint64_t sA, uint32_t L_dec, uint64_t sB) {
+    const uint32_t lane = lane_id();
+    const uint32_t wpc = blockDim.x >> 5;
+    for (uint32_t row = blockIdx.x * wpc + (threadIdx.x >> 5); row < N; row += gridDim.x * wpc) {
+        const uint32_t *ar = A + row * sA;
+        const uint32_t pad = 32u * G - L;
+        uint32_t x[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const uint32_t i = g * 32u + lane;
+            x[g] = (i >= pad) ? ar[i - pad] : 0u;
+        }
+        char *out = B + row * sB;
+        for (uint32_t start = 0; start < L_dec; start += 9u) {
+            uint32_t cin = 0u;
+            uint32_t prev_hi = 0u;   // hi(x[lane-1 of flattened]*1e9) for lane 0 of group g
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const uint64_t t = (uint64_t)x[g] * kTen9;
+                const uint32_t lo = (uint32_t)t;
+                const uint32_t hi = (uint32_t)(t >> 32);
+                uint32_t y = __shfl_up_sync(0xffffffffu, hi, 1);
+                if (lane == 0) y = prev_hi;
+                prev_hi = __shfl_sync(0xffffffffu, hi, 31);
+                bool gg, pp;
+                const uint32_t s = raw_limb<false>(lo, y, gg, pp);
+                const uint32_t gm = __ballot_sync(0xffffffffu, gg);
+                const uint32_t pm = __ballot_sync(0xffffffffu, pp);
+                const GroupCarry gc = resolve_group(gm, pm, cin);
+                cin = gc.carry_out;
+                x[g] = s + ((gc.carry_in_mask >> lane) & 1u);
+            }
+            const uint32_t chunk = prev_hi + cin;   // overflow out of the top limb
+            const uint32_t cnt = min(9u, L_dec - start);
+            if (lane < cnt) {
+                // lane m-1 writes place start+m
+                const uint32_t m = lane + 1u;
+                uint32_t v = chunk;
+                for (uint32_t e = 9; e > m; --e) v /= 10u;
+                const uint32_t k = start + m;
+                out[NATURAL ? (k - 1u) : (L_dec - k)] = (char)('0' + v % 10u);
+            }
+        }
+    }
+}
+
+template <bool NATURAL>
+void decimal_rows(const uint32_t *A, char *B, uint32_t N, uint32_t L, uint64_t sA, uint32_t L_dec,
+                  uint64_t sB) {
+    if (N == 0u || L == 0u || L_dec == 0u) return;
+    cudaStream_t st = current_stream();
+    const unsigned gt = grid_for(N, 128, kNumSMs * 32);
+    const unsigned gw = grid_for(N, 4, kNumSMs * 32);
+    if (L <= 8u) k_decimal_thread<8, NATURAL><<<gt, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    else if (L <= 16u) k_decimal_thread<16, NATURAL><<<gt, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    else if (L <= 32u) k_decimal_thread<32, NATURAL><<<gt, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    else if (L <= 64u) k_decimal_thread<64, NATURAL><<<gt, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    else if (L <= 256u) k_decimal_warp<8, NATURAL><<<gw, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    else if (L <= 1024u) k_decimal_warp<32, NATURAL><<<gw, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    else k_decimal_warp<64, NATURAL><<<gw, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
+    count_launch();
+}
+
+// dst row (2*row + off) limb j = bits [shift + 32j, shift + 32j + 32) of src row.
+__global__ void k_extract_shifted(const uint32_t *__restrict__ src, uint64_t s_stride, uint32_t s_len,
+                                  uint32_t *__restrict__ dst, uint64_t d_stride, uint32_t d_len,
+                                  uint32_t rows, uint32_t shift, uint32_t off) {
+    const uint64_t total = (uint64_t)rows * d_len;
+    const uint32_t w = shift >> 5, b = shift & 31u;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t row = (uint32_t)(t / d_len);
+        const uint32_t j = (uint32_t)(t - (uint64_t)row * d_len);
+        const uint32_t *s = src + row * s_stride;
+        const uint32_t i = j + w;
+        uint32_t v = 0u;
+        if (i < s_len) {
+            v = s[i] >> b;
+            if (b != 0u && i + 1u < s_len) v |= s[i + 1u] << (32u - b);
+        }
+        dst[(uint64_t)(2u * row + off) * d_stride + j] = v;
+    }
+}
+
+// dst limb j = src limb j for j < d_len, top limb masked to `top_mask`.
+__global__ void k_extract_low(const uint32_t *__restrict__ src, uint64_t s_stride,
+                              uint32_t *__restrict__ dst, uint64_t d_stride, uint32_t d_len,
+                              uint32_t rows, uint32_t top_mask) {
+    const uint64_t total = (uint64_t)rows * d_len;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t row = (uint32_t)(t / d_len);
+        const uint32_t j = (uint32_t)(t - (uint64_t)row * d_len);
+        uint32_t v = src[row * s_stride + j];
+        if (j + 1u == d_len) v &= top_mask;
+        dst[row * d_stride + j] = v;
+    }
+}
+
+static void extract_shifted(const BatchMPArray &src, uint32_t *dst, uint32_t d_stride,
+                            uint32_t d_len, uint32_t rows, uint32_t shift, uint32_t off) {
+    if (d_len == 0u || rows == 0u) return;
+    const uint64_t total = (uint64_t)rows * d_len;
+    k_extract_shifted<<<grid_for(total, 256, kNumSMs * 32), 256, 0, current_stream()>>>(
+        src.data, src.stride, src.length, dst, d_stride, d_len, rows, shift, off);
+    count_launch();
+}
+
+static void extract_low(const BatchMPArray &src, uint32_t *dst, uint32_t d_stride, uint32_t d_len,
+                        uint32_t rows, uint32_t valid_bits) {
+    if (d_len == 0u || rows == 0u) return;
+    uint32_t mask = 0xffffffffu;
+    if (valid_bits & 31u) mask = (1u << (valid_bits & 31u)) - 1u;
+    const uint64_t total = (uint64_t)rows * d_len;
+    k_extract_low<<<grid_for(total, 256, kNumSMs * 32), 256, 0, current_stream()>>>(
+        src.data, src.stride, dst, d_stride, d_len, rows, mask);
+    count_launch();
+}
+
+constexpr double kLog2_10 = 3.32192809488736234787;   // convert_decimal.cu:15
+constexpr uint32_t kMarginBits = 34u;                 // convert_decimal.cu:16
+
+static uint32_t bits_for_digits(uint32_t digits) {
+    return (uint32_t)(ceil((double)digits * kLog2_10) + (double)kMarginBits);
+}
+
+static uint32_t levels_for_shape(uint32_t total, uint32_t leaf) {
+    if (leaf == 0u || total == 0u || total % leaf != 0u) return UINT32_MAX;
+    uint32_t ratio = total / leaf, levels = 0u;
+    while (ratio > 1u && (ratio & 1u) == 0u) {
+        ratio >>= 1;
+        ++levels;
+    }
+    return ratio == 1u ? levels : UINT32_MAX;
+}
+
+// 5^e as little-endian limbs (host).
+static std::vector<uint32_t> pow5(uint32_t e) {
+    std::vector<uint32_t> v(1, 1u);
+    for (uint32_t i = 0; i < e; ++i) {
+        uint64_t c = 0;
+        for (auto &w : v) {
+            const uint64_t t = (uint64_t)w * 5u + c;
+            w = (uint32_t)t;
+            c = t >> 32;
+        }
+        if (c) v.push_back((uint32_t)c);
+    }
+    return v;
+}
+
+struct DevBuf {
+    uint32_t *p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t words) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        return words ? cudaMalloc(&p, words * 4) : cudaSuccess;
+    }
+};
+
+}  // namespace gpupi
+
+using namespace gpupi;
+
+void batch_decimal_naive(const uint32_t *A, char *B, uint32_t N, int L_limb, uint32_t stride_A,
+                         int L_dec, uint32_t stride_B) {
+    if (N == 0u || L_limb <= 0 || L_dec <= 0 || L_limb > BATCH_DECIMAL_NAIVE_L_LIMB_MAX) return;
+    decimal_rows<false>(A, B, N, (uint32_t)L_limb, stride_A, (uint32_t)L_dec, stride_B);
+}
+
+cudaError_t convert_decimal_precompute_powers(BatchMPContext *ctx, ConvertDecimalPowerTable *table,
+                                              uint32_t leaf_digits, uint32_t levels) {
+    if (ctx == nullptr || table == nullptr || leaf_digits == 0u) return cudaErrorInvalidValue;
+    table->powers = nullptr;
+    table->levels = 0u;
+    table->leaf_digits = leaf_digits;
+    if (levels == 0u) return cudaSuccess;
+    BatchMPArray *powers = new (std::nothrow) BatchMPArray[levels];
+    if (powers == nullptr) return cudaErrorMemoryAllocation;
+    for (uint32_t i = 0; i < levels; ++i) powers[i] = BatchMPArray{};
+    auto fail = [&](uint32_t made, cudaError_t e) {
+        for (uint32_t i = 0; i < made; ++i) batch_mp_array_release(powers[i]);
+        delete[] powers;
+        return e;
+    };
+    const std::vector<uint32_t> base = pow5(leaf_digits);
+    powers[0] = batch_mp_array_create(1u, (uint32_t)base.size());
+    if (powers[0].data == nullptr) return fail(0, cudaErrorMemoryAllocation);
+    cudaError_t err = cudaMemcpyAsync(powers[0].data, base.data(), base.size() * 4,
+                                      cudaMemcpyHostToDevice, current_stream());
+    if (err == cudaSuccess) err = cudaStreamSynchronize(current_stream());
+    if (err != cudaSuccess) return fail(1, err);
+    for (uint32_t l = 1; l < levels; ++l) {
+        BatchMPArray next = batch_mp_array_create(1u, powers[l - 1].length * 2u);
+        if (next.data == nullptr) return fail(l, cudaErrorMemoryAllocation);
+        err = batch_mp_mul(ctx, powers[l - 1], powers[l - 1], next);
+        if (err == cudaSuccess) err = next.compact(ctx);
+        if (err != cudaSuccess) {
+            batch_mp_array_release(next);
+            return fail(l, err);
+        }
+        powers[l] = next;
+    }
+    table->powers = powers;
+    table->levels = levels;
+    return cudaSuccess;
+}
+
+void convert_decimal_release_powers(ConvertDecimalPowerTable *table) {
+    if (table == nullptr) return;
+    if (table->powers != nullptr) {
+        for (uint32_t i = 0; i < table->levels; ++i) batch_mp_array_release(table->powers[i]);
+        delete[] table->powers;
+    }
+    table->powers = nullptr;
+    table->levels = 0u;
+}
+
+cudaError_t convert_decimal_equal_split(BatchMPContext *ctx, BatchMPArray input, uint32_t input_bits,
+                                        uint32_t total_digits, uint32_t leaf_digits,
+                                        const ConvertDecimalPowerTable *table, char *output_digits) {
+    if (ctx == nullptr || output_digits == nullptr || input.batch_size != 1u || input.data == nullptr)
+        return cudaErrorInvalidValue;
+    const uint32_t levels = levels_for_shape(total_digits, leaf_digits);
+    if (levels == UINT32_MAX || table == nullptr || table->leaf_digits != leaf_digits ||
+        table->levels != levels)
+        return cudaErrorInvalidValue;
+    cudaStream_t st = current_stream();
+
+    std::vector<uint32_t> digs(levels + 1), bits(levels + 1), limbs(levels + 1);
+    digs[0] = total_digits;
+    bits[0] = input_bits;
+    limbs[0] = input.length;
+    for (uint32_t l = 1; l <= levels; ++l) {
+        digs[l] = digs[l - 1] >> 1;
+        bits[l] = bits_for_digits(digs[l]);
+        limbs[l] = (bits[l] + 31u) / 32u;
+    }
+
+    // Buffers reused across levels: two row sets (ping/pong), mantissa, product.
+    size_t max_rows_words = 0, max_mant = 0, max_prod = 0;
+    for (uint32_t l = 0; l < levels; ++l) {
+        const size_t rows = (size_t)1 << l;
+        max_rows_words = std::max(max_rows_words, rows * 2 * limbs[l + 1]);
+        const uint32_t mant_len = (bits[l] - digs[l + 1] + 31u) / 32u;
+        max_mant = std::max(max_mant, rows * mant_len);
+        max_prod = std::max(max_prod, rows * (mant_len + table->powers[levels - 1 - l].length));
+    }
+    DevBuf ping, pong, mant, prod;
+    BatchMPArray current = input;
+    if (levels == 0u) {
+        const uint32_t need = bits_for_digits(total_digits);
+        const uint32_t nl = (need + 31u) / 32u;
+        if (input_bits < need) return cudaErrorInvalidValue;
+        cudaError_t err = ping.alloc(nl);
+        if (err != cudaSuccess) return err;
+        cudaMemsetAsync(ping.p, 0, (size_t)nl * 4, st);
+        // single row: dst row index 2*0+0 = 0
+        extract_shifted(input, ping.p, nl, nl, 1u, input_bits - need, 0u);
+        current = BatchMPArray{ping.p, nl, 1u, nl};
+    } else {
+        cudaError_t err = ping.alloc(max_rows_words);
+        if (err == cudaSuccess) err = pong.alloc(max_rows_words);
+        if (err == cudaSuccess) err = mant.alloc(max_mant);
+        if (err == cudaSuccess) err = prod.alloc(max_prod);
+        if (err != cudaSuccess) return err;
+        DevBuf *bufs[2] = {&ping, &pong};
+        for (uint32_t l = 0; l < levels; ++l) {
+            const uint32_t d = digs[l + 1];
+            const uint32_t cb = bits[l + 1];
+            const uint32_t B = bits[l];
+            if (current.length < limbs[l]) return cudaErrorInvalidValue;
+            if (B <= d || B < cb) return cudaErrorInvalidValue;
+            const uint32_t rows = current.batch_size;
+            const uint32_t nl = limbs[l + 1];
+            uint32_t *next = bufs[l & 1]->p;
+            // every child limb is written by the two extractions below
+            extract_shifted(current, next, nl, nl, rows, B - cb, 0u);
+            const uint32_t mant_bits = B - d;
+            const uint32_t mant_len = (mant_bits + 31u) / 32u;
+            extract_low(current, mant.p, mant_len, mant_len, rows, mant_bits);
+            const BatchMPArray &pw = table->powers[levels - 1 - l];
+            BatchMPArray mA{mant.p, mant_len, rows, mant_len};
+            BatchMPArray pB{pw.data, pw.length, rows, 0u};
+            BatchMPArray pC{prod.p, mant_len + pw.length, rows, mant_len + pw.length};
+            err = batch_mp_mul(ctx, mA, pB, pC);
+            if (err != cudaSuccess) return err;
+            extract_shifted(pC, next, nl, nl, rows, mant_bits - cb, 1u);
+            current = BatchMPArray{next, nl, rows * 2u, nl};
+        }
+    }
+    const uint32_t leaf_bits = (levels == 0u) ? bits_for_digits(total_digits) : bits[levels];
+    const uint32_t align = current.length * 32u - leaf_bits;
+    DevBuf aligned;
+    cudaError_t err = aligned.alloc((size_t)current.batch_size * current.length);
+    if (err != cudaSuccess) return err;
+    batch_shift_bits(current.data, aligned.p, current.batch_size, current.length, current.length,
+                     current.stride, current.length, (int32_t)align);
+    decimal_rows<true>(aligned.p, output_digits, current.batch_size, current.length, current.length,
+                       leaf_digits, leaf_digits);
+    err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    return err;
+}

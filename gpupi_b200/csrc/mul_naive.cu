@@ -1,0 +1,182 @@
+// Batched schoolbook multiplication (gpupi batch_mul_naive.cu:8-273).
+//
+// Two shapes:
+//   * k_school_thread<MA, MB>: one thread per product for operands of at most
+//     MA x MB limbs (the bottom levels of the splitting tree: 3..16-limb rows
+//     in batches of millions).  Register arrays, fully unrolled MACs.
+//   * k_school_cols: one CTA per product, 256 threads x 4 consecutive output
+//     columns.  Each column sum sum_i a_i b_(k-i) is accumulated exactly in a
+//     3-word register with mad.lo.cc / madc.hi.cc / addc (3 instructions per
+//     32x32 product), then the 96-bit column sums are carried into limbs with
+//     the same chunk/ballot carry as the NTT's CRT stage.  L_a + L_b <= 1024.
+// Both are IMAD-bound; algorithmic work = L_a * L_b 32x32->64 products.
+#include "common.cuh"
+#include "carry_tile.cuh"
+#include "batch_mul_naive.h"
+
+namespace gpupi {
+
+template <int MA, int MB>
+__global__ void __launch_bounds__(128) k_school_thread(const uint32_t *__restrict__ A,
+                                                       const uint32_t *__restrict__ B,
+                                                       uint32_t *__restrict__ C, uint32_t N,
+                                                       uint32_t La, uint32_t Lb, uint64_t sA,
+                                                       uint64_t sB, uint64_t sC) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < N;
+         row += gridDim.x * blockDim.x) {
+        uint32_t a[MA], b[MB], o[MA + MB];
+        const uint32_t *ar = A + row * sA;
+        const uint32_t *br = B + row * sB;
+#pragma unroll
+        for (int i = 0; i < MA; ++i) a[i] = (i < (int)La) ? ar[i] : 0u;
+#pragma unroll
+        for (int j = 0; j < MB; ++j) b[j] = (j < (int)Lb) ? br[j] : 0u;
+#pragma unroll
+        for (int k = 0; k < MA + MB; ++k) o[k] = 0u;
+#pragma unroll
+        for (int i = 0; i < MA; ++i) {
+            uint32_t carry = 0u;
+#pragma unroll
+            for (int j = 0; j < MB; ++j) {
+                const uint64_t t = (uint64_t)a[i] * b[j] + o[i + j] + carry;
+                o[i + j] = (uint32_t)t;
+                carry = (uint32_t)(t >> 32);
+            }
+            o[i + MB] = carry;
+        }
+        uint32_t *cr = C + row * sC;
+        const uint32_t Lc = La + Lb;
+#pragma unroll
+        for (int k = 0; k < MA + MB; ++k)
+            if (k < (int)Lc) cr[k] = o[k];
+    }
+}
+
+__device__ __forceinline__ void mac3(uint32_t &c0, uint32_t &c1, uint32_t &c2, uint32_t a, uint32_t b) {
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(c0), "+r"(c1), "+r"(c2)
+        : "r"(a), "r"(b));
+}
+
+constexpr int kSchoolThreads = 256;
+constexpr int kSchoolV = 4;
+constexpr int kSchoolMaxL = kSchoolThreads * kSchoolV;   // 1024 output limbs
+
+__global__ void __launch_bounds__(kSchoolThreads) k_school_cols(const uint32_t *__restrict__ A,
+                                                                const uint32_t *__restrict__ B,
+                                                                uint32_t *__restrict__ C, uint32_t N,
+                                                                uint32_t La, uint32_t Lb, uint64_t sA,
+                                                                uint64_t sB, uint64_t sC) {
+    // a[0..La), bpad[j + kPad] = b_j (zero outside [0, Lb))
+    __shared__ uint32_t sa[kSchoolMaxL];
+    __shared__ uint32_t sb[kSchoolMaxL + kSchoolMaxL + 8];
+    __shared__ uint32_t sg[kSchoolThreads / 32], sp[kSchoolThreads / 32];
+    const uint32_t kPad = La + 4;
+    const uint32_t Lc = La + Lb;
+    for (uint32_t row = blockIdx.x; row < N; row += gridDim.x) {
+        const uint32_t *ar = A + row * sA;
+        const uint32_t *br = B + row * sB;
+        for (uint32_t i = threadIdx.x; i < La; i += blockDim.x) sa[i] = ar[i];
+        for (uint32_t j = threadIdx.x; j < kPad + Lb + 8; j += blockDim.x)
+            sb[j] = (j >= kPad && j - kPad < Lb) ? br[j - kPad] : 0u;
+        __syncthreads();
+        const uint32_t k0 = threadIdx.x * kSchoolV;
+        uint32_t c[kSchoolV][3];
+#pragma unroll
+        for (int v = 0; v < kSchoolV; ++v) c[v][0] = c[v][1] = c[v][2] = 0u;
+        if (k0 < Lc) {
+            // terms a_i * b_(k-i) for k in [k0, k0+4): i in [max(0, k0+1-Lb), min(La-1, k0+3)]
+            const int ilo = max(0, (int)k0 + 1 - (int)Lb);
+            const int ihi = min((int)La - 1, (int)k0 + kSchoolV - 1);
+            for (int i = ilo; i <= ihi; ++i) {
+                const uint32_t ai = sa[i];
+                const uint32_t *bw = sb + kPad + k0 - i;   // bw[v] = b_(k0+v-i)
+#pragma unroll
+                for (int v = 0; v < kSchoolV; ++v) mac3(c[v][0], c[v][1], c[v][2], ai, bw[v]);
+            }
+        }
+        uint32_t S[kSchoolV + 3];
+        chunk_sum3<kSchoolV>(c, S);
+        uint32_t H[3];
+        H[0] = __shfl_up_sync(0xffffffffu, S[kSchoolV], 1);
+        H[1] = __shfl_up_sync(0xffffffffu, S[kSchoolV + 1], 1);
+        H[2] = __shfl_up_sync(0xffffffffu, S[kSchoolV + 2], 1);
+        __shared__ uint32_t spill[kSchoolThreads / 32][3];
+        if (lane_id() == 31) {
+            spill[threadIdx.x >> 5][0] = S[kSchoolV];
+            spill[threadIdx.x >> 5][1] = S[kSchoolV + 1];
+            spill[threadIdx.x >> 5][2] = S[kSchoolV + 2];
+        }
+        __syncthreads();
+        if (lane_id() == 0) {
+            const int w = threadIdx.x >> 5;
+            H[0] = w ? spill[w - 1][0] : 0u;
+            H[1] = w ? spill[w - 1][1] : 0u;
+            H[2] = w ? spill[w - 1][2] : 0u;
+        }
+        uint32_t X[kSchoolV];
+        const uint32_t g = chunk_add_spill<kSchoolV>(S, H, X);
+        bool p = true;
+#pragma unroll
+        for (int v = 0; v < kSchoolV; ++v) p = p && (X[v] == 0xffffffffu);
+        const BlockCarry bc = block_resolve<kSchoolThreads / 32>(g != 0u, p, sg, sp);
+        chunk_increment<kSchoolV>(X, bc.cin);
+        uint32_t *cr = C + row * sC;
+#pragma unroll
+        for (int v = 0; v < kSchoolV; ++v)
+            if (k0 + v < Lc) cr[k0 + v] = X[v];
+        __syncthreads();
+    }
+}
+
+// Thread-per-product size classes.
+template <int MA, int MB>
+static void launch_thread(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La,
+                          uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC, cudaStream_t st) {
+    k_school_thread<MA, MB><<<grid_for(N, 128, kNumSMs * 32), 128, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+    count_launch();
+}
+
+bool school_thread_fits(uint32_t La, uint32_t Lb) {
+    return (La <= 16u && Lb <= 16u);
+}
+
+void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La,
+                uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC) {
+    cudaStream_t st = current_stream();
+    if (N == 0u || La + Lb == 0u) return;
+    if (La == 0u || Lb == 0u) {
+        cudaMemset2DAsync(C, sC * 4, 0, (size_t)(La + Lb) * 4, N, st);
+        return;
+    }
+    // keep the longer operand as A for the register kernels
+    if (La < Lb) {
+        std::swap(A, B);
+        std::swap(La, Lb);
+        std::swap(sA, sB);
+    }
+    if (La <= 4u && Lb <= 4u) {
+        launch_thread<4, 4>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else if (La <= 8u && Lb <= 8u) {
+        launch_thread<8, 8>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else if (La <= 16u && Lb <= 8u) {
+        launch_thread<16, 8>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else if (La <= 16u && Lb <= 16u) {
+        launch_thread<16, 16>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else {
+        k_school_cols<<<grid_for(N, 1, kNumSMs * 16), kSchoolThreads, 0, st>>>(A, B, C, N, La, Lb, sA,
+                                                                             sB, sC);
+        count_launch();
+    }
+}
+
+}  // namespace gpupi
+
+void batch_mul_naive(uint32_t *A, uint32_t *B, uint32_t *ret, int N, int L_a, int L_b, int stride_A,
+                     int stride_B, int stride_ret) {
+    if (N <= 0 || L_a < 0 || L_b < 0 || L_a + L_b > BATCH_MUL_NAIVE_L_MAX) return;
+    gpupi::school_mul(A, B, ret, (uint32_t)N, (uint32_t)L_a, (uint32_t)L_b, (uint32_t)stride_A,
+                      (uint32_t)stride_B, (uint32_t)stride_ret);
+}

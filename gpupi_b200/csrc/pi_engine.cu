@@ -1,0 +1,771 @@
+// Chudnovsky pi pipeline driver (gpupi pi_bs_gpu.cu:36-131, 504-792,
+// 1143-1685, 2073-2431).
+//
+// Host C++ drives the same sequence of batched operations as the reference,
+// with the same operand lengths (including every compact()-derived length),
+// so every intermediate integer, the RET value and the digits are identical.
+// All limb work is done by this library's kernels on the current stream.
+// Temporary device buffers come from the stream-ordered allocator
+// (cudaMallocAsync), so per-level allocation costs no device synchronisation.
+#include "common.cuh"
+#include "batch_arith.h"
+#include "batch_mul_naive.h"
+#include "convert_decimal.h"
+#include "pi_engine.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+namespace gpupi {
+
+// ---------------------------------------------------------------------------
+// Leaves (pi_bs_gpu.cu:17-131): P (3 limbs), Q (4), R (6) per term, after the
+// same common-factor reductions by 5, 3, 23, 29.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reduce_pair(uint32_t &a, uint32_t &b) {
+    if (a % 3u == 0u && b % 3u == 0u) { a /= 3u; b /= 3u; }
+    if (a % 5u == 0u && b % 5u == 0u) { a /= 5u; b /= 5u; }
+    if (a % 23u == 0u && b % 23u == 0u) { a /= 23u; b /= 23u; }
+    if (a % 29u == 0u && b % 29u == 0u) { a /= 29u; b /= 29u; }
+}
+
+template <int L>
+__device__ __forceinline__ void mul_small_into(uint32_t (&x)[L], uint32_t m) {
+    uint32_t c = 0u;
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        const uint64_t t = (uint64_t)x[j] * m + c;
+        x[j] = (uint32_t)t;
+        c = (uint32_t)(t >> 32);
+    }
+}
+
+template <bool HEAD>
+__global__ void k_leaves(uint32_t *P, uint32_t *Q, uint32_t *R, uint32_t rows) {
+    for (uint32_t i2 = blockIdx.x * blockDim.x + threadIdx.x; i2 < rows; i2 += gridDim.x * blockDim.x) {
+        const uint32_t i = HEAD ? i2 * 17u + 16u : i2 + (i2 >> 4);
+        uint32_t p1 = 6u * i + 1u, p2 = 2u * i + 1u, p3 = 6u * i + 5u;
+        uint32_t q1 = i + 1u, q2 = i + 1u, q3 = i + 1u;
+        uint32_t q4 = 640320u >> 6, q5 = 40020u >> 2;
+        const uint32_t q6 = 426880u >> 7;
+        const uint64_t r1 = 545140134ull * i + 13591409ull;
+        if (p1 % 5u == 0u && q1 % 5u == 0u) { p1 /= 5u; q1 /= 5u; }
+        if (p1 % 5u == 0u && q2 % 5u == 0u) { p1 /= 5u; q2 /= 5u; }
+        if (p1 % 5u == 0u && q3 % 5u == 0u) { p1 /= 5u; q3 /= 5u; }
+        reduce_pair(p1, q4);
+        reduce_pair(p1, q5);
+        reduce_pair(p2, q4);
+        reduce_pair(p2, q5);
+        reduce_pair(p3, q4);
+        reduce_pair(p3, q5);
+        uint32_t pp[3] = {p1, 0u, 0u};
+        mul_small_into<3>(pp, p2);
+        mul_small_into<3>(pp, p3);
+        uint32_t qq[4] = {q1, 0u, 0u, 0u};
+        mul_small_into<4>(qq, q2);
+        mul_small_into<4>(qq, q3);
+        mul_small_into<4>(qq, q4);
+        mul_small_into<4>(qq, q5);
+        mul_small_into<4>(qq, q6);
+        uint32_t rr[6] = {(uint32_t)r1, (uint32_t)(r1 >> 32), 0u, 0u, 0u, 0u};
+        mul_small_into<6>(rr, q1);
+        mul_small_into<6>(rr, q2);
+        mul_small_into<6>(rr, q3);
+        mul_small_into<6>(rr, q4);
+        mul_small_into<6>(rr, q5);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) P[(uint64_t)i2 * 3 + k] = pp[k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) Q[(uint64_t)i2 * 4 + k] = qq[k];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) R[(uint64_t)i2 * 6 + k] = rr[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage profiler (pi_bs_gpu.cu:133-242): one event pair per op, synchronised.
+// ---------------------------------------------------------------------------
+struct Profiler {
+    std::vector<StageEntry> entries;
+    bool on = false;
+};
+
+template <typename Fn>
+static cudaError_t stage(Profiler *pr, const char *kind, const char *label, uint32_t n1, uint32_t batch,
+                         uint32_t lhs, uint32_t rhs, bool uses_ntt, Fn &&fn) {
+    if (pr == nullptr || !pr->on) return fn();
+    cudaStream_t st = current_stream();
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+    cudaError_t err = fn();
+    if (err == cudaSuccess) err = cudaEventRecord(b, st);
+    if (err == cudaSuccess) err = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, a, b);
+    if (err == cudaSuccess && pr->entries.size() < 2048) {
+        StageEntry e;
+        e.kind = kind;
+        e.label = label;
+        e.n1 = n1;
+        e.batch = batch;
+        e.lhs = lhs;
+        e.rhs = rhs;
+        e.ms = ms;
+        e.uses_ntt = uses_ntt;
+        pr->entries.push_back(e);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return err;
+}
+
+#define TRY(x)                                   \
+    do {                                         \
+        cudaError_t _e = (x);                    \
+        if (_e != cudaSuccess) return _e;        \
+    } while (0)
+
+static cudaError_t p_mul(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, BatchMPArray B, BatchMPArray C,
+                         const char *label, uint32_t n1) {
+    return stage(pr, "mul", label, n1, A.batch_size, A.length, B.length,
+                 (size_t)A.length + B.length > (size_t)BATCH_MUL_NAIVE_L_MAX,
+                 [&]() { return batch_mp_mul(ctx, A, B, C); });
+}
+static cudaError_t p_compact(BatchMPContext *ctx, Profiler *pr, BatchMPArray &A, const char *label, uint32_t n1) {
+    return stage(pr, "compact", label, n1, A.batch_size, A.length, 0, false, [&]() { return A.compact(ctx); });
+}
+static cudaError_t p_shift_addsub(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, BatchMPArray B,
+                                  BatchMPArray C, uint32_t shift, bool sub, uint32_t n1) {
+    return stage(pr, sub ? "sub" : "add", sub ? "R*Q<<15n-P*R" : "R*Q<<15n+P*R", n1, A.batch_size, A.length,
+                 B.length, false, [&]() {
+                     return sub ? batch_mp_shift_sub(ctx, A, B, shift, C) : batch_mp_shift_add(ctx, A, B, shift, C);
+                 });
+}
+static cudaError_t p_exactdiv(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, const char *label, uint32_t d,
+                              uint32_t n1) {
+    return stage(pr, "exactdiv", label, n1, A.batch_size, A.length, 0, false,
+                 [&]() { return batch_mp_exactdiv_small(ctx, A, d); });
+}
+static cudaError_t p_add(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, BatchMPArray B, BatchMPArray C,
+                         const char *label, uint32_t dg) {
+    return stage(pr, "add", label, dg, A.batch_size, A.length, B.length, false,
+                 [&]() { return batch_mp_add(ctx, A, B, C); });
+}
+static cudaError_t p_sub(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, BatchMPArray B, BatchMPArray C,
+                         const char *label, uint32_t dg) {
+    return stage(pr, "sub", label, dg, A.batch_size, A.length, B.length, false,
+                 [&]() { return batch_mp_sub(ctx, A, B, C); });
+}
+static cudaError_t p_add_small(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, uint32_t v, BatchMPArray C,
+                               const char *label, uint32_t dg) {
+    return stage(pr, "add", label, dg, A.batch_size, A.length, 1, false,
+                 [&]() { return batch_mp_add_small(ctx, A, v, C); });
+}
+static cudaError_t p_mul_small(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, uint32_t v, BatchMPArray C,
+                               const char *label, uint32_t dg) {
+    return stage(pr, "mul_small", label, dg, A.batch_size, A.length, 1, false,
+                 [&]() { return batch_mp_mul_small(ctx, A, v, C); });
+}
+static cudaError_t p_shift(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, BatchMPArray B, int32_t s,
+                           const char *label, uint32_t dg) {
+    return stage(pr, "shift", label, dg, A.batch_size, A.length, 0, false,
+                 [&]() { return batch_mp_shift_bits(ctx, A, B, s); });
+}
+
+// Stream-ordered device buffer.
+struct Buf {
+    uint32_t *p = nullptr;
+    Buf() = default;
+    Buf(const Buf &) = delete;
+    Buf &operator=(const Buf &) = delete;
+    ~Buf() { reset(); }
+    void reset() {
+        if (p) cudaFreeAsync(p, current_stream());
+        p = nullptr;
+    }
+    cudaError_t alloc(size_t words) {
+        reset();
+        if (words == 0) words = 1;
+        return cudaMallocAsync(&p, words * 4, current_stream());
+    }
+    void swap(Buf &o) { std::swap(p, o.p); }
+};
+
+static const uint32_t kDivLo = 830297u;       // pi_bs_gpu.cu:147
+static const uint32_t kDivHi = 156590819u;    // pi_bs_gpu.cu:148
+
+// ---------------------------------------------------------------------------
+// Binary splitting of 17N terms (pi_bs_gpu.cu:504-792).
+// Q and R (batch 1) are returned in qbuf/rbuf with their compacted lengths.
+// ---------------------------------------------------------------------------
+static cudaError_t binary_split(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &qbuf, BatchMPArray &Q,
+                                Buf &rbuf, BatchMPArray &R) {
+    if (N == 0u || (N & (N - 1u)) != 0u) return cudaErrorInvalidValue;
+    cudaStream_t st = current_stream();
+    const uint32_t n = N * 16u;
+    Buf p0, q0, r0, pb, qb, rb, pn, qn, rn, r1b, r2b;
+    TRY(p0.alloc((size_t)N * 3));
+    TRY(q0.alloc((size_t)N * 4));
+    TRY(r0.alloc((size_t)N * 6));
+    TRY(pb.alloc((size_t)n * 3));
+    TRY(qb.alloc((size_t)n * 4));
+    TRY(rb.alloc((size_t)n * 6));
+    TRY(stage(pr, "leaf", "construct_leaf", N * 17u, N, 3, 0, false, [&]() {
+        k_leaves<true><<<grid_for(N, 128, 65535), 128, 0, st>>>(p0.p, q0.p, r0.p, N);
+        count_launch();
+        return cudaGetLastError();
+    }));
+    TRY(stage(pr, "leaf", "construct_leaf", N * 17u, n, 3, 0, false, [&]() {
+        k_leaves<false><<<grid_for(n, 128, 65535), 128, 0, st>>>(pb.p, qb.p, rb.p, n);
+        count_launch();
+        return cudaGetLastError();
+    }));
+    const BatchMPArray P0{p0.p, 3, N, 3}, Q0{q0.p, 4, N, 4}, R0{r0.p, 6, N, 6};
+    BatchMPArray P{pb.p, 3, n, 3};
+    Q = BatchMPArray{qb.p, 4, n, 4};
+    R = BatchMPArray{rb.p, 6, n, 6};
+
+    for (uint32_t n1 = n; n1 > 1u; n1 >>= 1) {
+        const bool subtract = (n1 == n) || (n1 == (n >> 4));
+        const uint32_t ignore = (n1 <= N) ? 1u : 0u;
+        const uint32_t half = n1 / 2u;
+        BatchMPArray P_even{P.data, P.length, half - ignore, P.stride * 2};
+        BatchMPArray P_odd{P.data + P.stride, P.length, half - ignore, P.stride * 2};
+        BatchMPArray Pn{nullptr, P.length * 2u, half - ignore, P.length * 2u};
+        if (P_odd.batch_size > 0u) {
+            TRY(pn.alloc((size_t)Pn.batch_size * Pn.stride));
+            Pn.data = pn.p;
+            TRY(p_mul(ctx, pr, P_even, P_odd, Pn, "P", n1));
+            TRY(p_compact(ctx, pr, Pn, "P", n1));
+        } else {
+            pn.reset();
+            Pn = BatchMPArray{nullptr, 0, 0, 0};
+        }
+        BatchMPArray Q_even{Q.data, Q.length, half, Q.stride * 2};
+        BatchMPArray Q_odd{Q.data + Q.stride, Q.length, half, Q.stride * 2};
+        BatchMPArray Qn{nullptr, Q.length * 2u, half, Q.length * 2u};
+        TRY(qn.alloc((size_t)half * Qn.stride));
+        Qn.data = qn.p;
+        TRY(p_mul(ctx, pr, Q_even, Q_odd, Qn, "Q", n1));
+        TRY(p_compact(ctx, pr, Qn, "Q", n1));
+        BatchMPArray R_even{R.data, R.length, half, R.stride * 2};
+        BatchMPArray R_odd{R.data + R.stride, R.length, half, R.stride * 2};
+        BatchMPArray R1{nullptr, R.length + Q.length, half, R.length + Q.length};
+        TRY(r1b.alloc((size_t)half * R1.stride));
+        R1.data = r1b.p;
+        TRY(p_mul(ctx, pr, R_even, Q_odd, R1, "R*Q", n1));
+        const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
+        BatchMPArray R2{nullptr, R.length + P.length, half, R.length + P.length};
+        TRY(r2b.alloc((size_t)half * R2.stride));
+        R2.data = r2b.p;
+        P_even.batch_size = half;
+        TRY(p_mul(ctx, pr, P_even, R_odd, R2, "P*R", n1));
+        const uint32_t r1_shifted = R1.length + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
+        const uint32_t rlen = std::max(r1_shifted, R2.length) + (subtract ? 0u : 1u);
+        BatchMPArray Rn{nullptr, rlen, half, rlen};
+        TRY(rn.alloc((size_t)half * rlen));
+        Rn.data = rn.p;
+        TRY(p_shift_addsub(ctx, pr, R1, R2, Rn, shift, subtract, n1));
+        TRY(p_compact(ctx, pr, Rn, "R", n1));
+        pb.swap(pn);
+        qb.swap(qn);
+        rb.swap(rn);
+        P = Pn;
+        Q = Qn;
+        R = Rn;
+        r1b.reset();
+        r2b.reset();
+        pn.reset();
+        qn.reset();
+        rn.reset();
+        if (n1 == (n >> 3)) {
+            // merge the head term of every 17-term block (pi_bs_gpu.cu:725-784)
+            BatchMPArray Pm{nullptr, P.length + P0.length, half, P.length + P0.length};
+            TRY(pn.alloc((size_t)half * Pm.stride));
+            Pm.data = pn.p;
+            TRY(p_mul(ctx, pr, P, P0, Pm, "P", n1));
+            TRY(p_compact(ctx, pr, Pm, "P", n1));
+            BatchMPArray Qm{nullptr, Q.length + Q0.length, half, Q.length + Q0.length};
+            TRY(qn.alloc((size_t)half * Qm.stride));
+            Qm.data = qn.p;
+            TRY(p_mul(ctx, pr, Q, Q0, Qm, "Q", n1));
+            TRY(p_compact(ctx, pr, Qm, "Q", n1));
+            BatchMPArray M1{nullptr, R.length + Q0.length, half, R.length + Q0.length};
+            TRY(r1b.alloc((size_t)half * M1.stride));
+            M1.data = r1b.p;
+            TRY(p_mul(ctx, pr, R, Q0, M1, "R*Q", n1));
+            BatchMPArray M2{nullptr, P.length + R0.length, half, P.length + R0.length};
+            TRY(r2b.alloc((size_t)half * M2.stride));
+            M2.data = r2b.p;
+            TRY(p_mul(ctx, pr, P, R0, M2, "P*R", n1));
+            const uint32_t ml = std::max(M1.length + 1u, M2.length) + 1u;
+            BatchMPArray Rm{nullptr, ml, half, ml};
+            TRY(rn.alloc((size_t)half * ml));
+            Rm.data = rn.p;
+            TRY(p_shift_addsub(ctx, pr, M1, M2, Rm, 15u, false, n1));
+            TRY(p_compact(ctx, pr, Rm, "R", n1));
+            TRY(p_exactdiv(ctx, pr, Pm, "P", kDivLo, n1));
+            TRY(p_exactdiv(ctx, pr, Pm, "P", kDivHi, n1));
+            TRY(p_compact(ctx, pr, Pm, "P", n1));
+            TRY(p_exactdiv(ctx, pr, Qm, "Q", kDivLo, n1));
+            TRY(p_exactdiv(ctx, pr, Qm, "Q", kDivHi, n1));
+            TRY(p_compact(ctx, pr, Qm, "Q", n1));
+            TRY(p_exactdiv(ctx, pr, Rm, "R", kDivLo, n1));
+            TRY(p_exactdiv(ctx, pr, Rm, "R", kDivHi, n1));
+            TRY(p_compact(ctx, pr, Rm, "R", n1));
+            pb.swap(pn);
+            qb.swap(qn);
+            rb.swap(rn);
+            P = Pm;
+            Q = Qm;
+            R = Rm;
+            r1b.reset();
+            r2b.reset();
+            pn.reset();
+            qn.reset();
+            rn.reset();
+        }
+    }
+    qbuf.swap(qb);
+    rbuf.swap(rb);
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// sqrt(10005) Pell iteration (pi_bs_gpu.cu:1346-1522): (p, q) <- (p^2 +
+// 10005 q^2, 2pq) from (4001, 40) while 7.5 * 2^k < digits.
+// ---------------------------------------------------------------------------
+static cudaError_t sqrt_10005(BatchMPContext *ctx, Profiler *pr, int target, Buf &pbuf, BatchMPArray &P,
+                              Buf &qbuf, BatchMPArray &Q) {
+    cudaStream_t st = current_stream();
+    TRY(pbuf.alloc(1));
+    TRY(qbuf.alloc(1));
+    const uint32_t p15 = 4001u, q15 = 40u;
+    TRY(cudaMemcpyAsync(pbuf.p, &p15, 4, cudaMemcpyHostToDevice, st));
+    TRY(cudaMemcpyAsync(qbuf.p, &q15, 4, cudaMemcpyHostToDevice, st));
+    TRY(cudaStreamSynchronize(st));
+    P = BatchMPArray{pbuf.p, 1, 1, 1};
+    Q = BatchMPArray{qbuf.p, 1, 1, 1};
+    double valid = 7.5;
+    while (valid < (double)target) {
+        valid *= 2;
+        const uint32_t sd = (uint32_t)valid;
+        Buf pq, nq, pp, qq, qq5, np;
+        BatchMPArray PQ{nullptr, P.length + Q.length, 1, P.length + Q.length};
+        TRY(pq.alloc(PQ.stride));
+        PQ.data = pq.p;
+        TRY(p_mul(ctx, pr, P, Q, PQ, "P*Q", sd));
+        TRY(p_compact(ctx, pr, PQ, "P*Q", sd));
+        BatchMPArray NQ{nullptr, PQ.length + 1u, 1, PQ.length + 1u};
+        TRY(nq.alloc(NQ.stride));
+        NQ.data = nq.p;
+        TRY(p_shift(ctx, pr, PQ, NQ, 1, "2*P*Q", sd));
+        TRY(p_compact(ctx, pr, NQ, "Q", sd));
+        BatchMPArray PP{nullptr, P.length * 2u, 1, P.length * 2u};
+        TRY(pp.alloc(PP.stride));
+        PP.data = pp.p;
+        TRY(p_mul(ctx, pr, P, P, PP, "P*P", sd));
+        TRY(p_compact(ctx, pr, PP, "P*P", sd));
+        BatchMPArray QQ{nullptr, Q.length * 2u, 1, Q.length * 2u};
+        TRY(qq.alloc(QQ.stride));
+        QQ.data = qq.p;
+        TRY(p_mul(ctx, pr, Q, Q, QQ, "Q*Q", sd));
+        TRY(p_compact(ctx, pr, QQ, "Q*Q", sd));
+        BatchMPArray Q5{nullptr, QQ.length + 1u, 1, QQ.length + 1u};
+        TRY(qq5.alloc(Q5.stride));
+        Q5.data = qq5.p;
+        TRY(p_mul_small(ctx, pr, QQ, 10005u, Q5, "10005*Q*Q", sd));
+        TRY(p_compact(ctx, pr, Q5, "10005*Q*Q", sd));
+        const uint32_t npl = std::max(PP.length, Q5.length) + 1u;
+        BatchMPArray NP{nullptr, npl, 1, npl};
+        TRY(np.alloc(npl));
+        NP.data = np.p;
+        TRY(p_add(ctx, pr, PP, Q5, NP, "P*P+10005*Q*Q", sd));
+        TRY(p_compact(ctx, pr, NP, "P", sd));
+        pbuf.swap(np);
+        qbuf.swap(nq);
+        P = NP;
+        Q = NQ;
+    }
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Exact host division for the inverse base case: (q, r) = divmod(2^e, v).
+// Knuth, TAOCP vol. 2, 4.3.1 Algorithm D on 32-bit limbs.
+// ---------------------------------------------------------------------------
+static void divmod_pow2(uint32_t e, std::vector<uint32_t> v, std::vector<uint32_t> &q, std::vector<uint32_t> &r) {
+    while (!v.empty() && v.back() == 0u) v.pop_back();
+    const size_t n = v.size();
+    std::vector<uint32_t> u(e / 32u + 2u, 0u);
+    u[e / 32u] = 1u << (e % 32u);
+    while (u.size() > 1 && u.back() == 0u) u.pop_back();
+    if (n == 0) {
+        q.clear();
+        r.clear();
+        return;
+    }
+    if (u.size() < n) {
+        q.assign(1, 0u);
+        r = u;
+        return;
+    }
+    const size_t m = u.size() - n;
+    q.assign(m + 1, 0u);
+    if (n == 1) {
+        uint64_t rem = 0;
+        for (size_t j = u.size(); j-- > 0;) {
+            const uint64_t cur = (rem << 32) | u[j];
+            q[j] = (uint32_t)(cur / v[0]);
+            rem = cur % v[0];
+        }
+        r.assign(1, (uint32_t)rem);
+        return;
+    }
+    const int s = __builtin_clz(v[n - 1]);
+    std::vector<uint32_t> vn(n), un(u.size() + 1, 0u);
+    for (size_t i = n - 1; i > 0; --i) vn[i] = (v[i] << s) | (s ? (uint32_t)((uint64_t)v[i - 1] >> (32 - s)) : 0u);
+    vn[0] = v[0] << s;
+    un[u.size()] = s ? (uint32_t)((uint64_t)u[u.size() - 1] >> (32 - s)) : 0u;
+    for (size_t i = u.size() - 1; i > 0; --i) un[i] = (u[i] << s) | (s ? (uint32_t)((uint64_t)u[i - 1] >> (32 - s)) : 0u);
+    un[0] = u[0] << s;
+    for (size_t j = m + 1; j-- > 0;) {
+        const uint64_t num = ((uint64_t)un[j + n] << 32) | un[j + n - 1];
+        uint64_t qhat = num / vn[n - 1];
+        uint64_t rhat = num % vn[n - 1];
+        while (qhat >= (1ull << 32) || qhat * vn[n - 2] > ((rhat << 32) | un[j + n - 2])) {
+            --qhat;
+            rhat += vn[n - 1];
+            if (rhat >= (1ull << 32)) break;
+        }
+        int64_t borrow = 0;
+        uint64_t carry = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const uint64_t prod = qhat * vn[i] + carry;
+            carry = prod >> 32;
+            const int64_t t = (int64_t)un[i + j] - (int64_t)(uint32_t)prod + borrow;
+            un[i + j] = (uint32_t)t;
+            borrow = t >> 32;
+        }
+        const int64_t t = (int64_t)un[j + n] - (int64_t)carry + borrow;
+        un[j + n] = (uint32_t)t;
+        if (t < 0) {
+            --qhat;
+            uint64_t c = 0;
+            for (size_t i = 0; i < n; ++i) {
+                const uint64_t sum = (uint64_t)un[i + j] + vn[i] + c;
+                un[i + j] = (uint32_t)sum;
+                c = sum >> 32;
+            }
+            un[j + n] += (uint32_t)c;
+        }
+        q[j] = (uint32_t)qhat;
+    }
+    r.assign(n, 0u);
+    for (size_t i = 0; i < n; ++i)
+        r[i] = (un[i] >> s) | (s ? (uint32_t)((uint64_t)un[i + 1] << (32 - s)) : 0u);
+    while (q.size() > 1 && q.back() == 0u) q.pop_back();
+    while (r.size() > 1 && r.back() == 0u) r.pop_back();
+}
+
+static BatchMPArray subview(const BatchMPArray &a, uint32_t start, uint32_t length) {
+    // make_subview, pi_bs_gpu.cu:1095-1110
+    if (start > a.length) start = a.length;
+    const uint32_t maxl = a.length - start;
+    if (length > maxl) length = maxl;
+    const uint32_t stride = (a.stride >= start) ? (a.stride - start) : 0u;
+    return BatchMPArray{a.data + start, length, a.batch_size, stride};
+}
+
+static cudaError_t shift_right_large(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, uint64_t bits,
+                                     BatchMPArray B, const char *label, uint32_t dg) {
+    // pi_bs_gpu.cu:1068-1093
+    const uint64_t limb_shift = bits / 32u;
+    if (limb_shift >= A.length) return cudaErrorInvalidValue;
+    const uint32_t ls = (uint32_t)limb_shift;
+    BatchMPArray pre{A.data + ls, A.length - ls, A.batch_size, A.stride - ls};
+    return p_shift(ctx, pr, pre, B, -(int32_t)(bits % 32u), label, dg);
+}
+
+// ---------------------------------------------------------------------------
+// Recursive inverse y ~ 2^L / x (pi_bs_gpu.cu:1145-1344).
+// y_out is allocated with x.length limbs; see the reference's python spec.
+// ---------------------------------------------------------------------------
+static const uint64_t kInverseCpuLimit = 32 * 1024;   // pi_bs_gpu.cu:1143
+
+static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPArray x, uint64_t L, Buf &ybuf,
+                                     BatchMPArray &y_out, uint32_t digits) {
+    cudaStream_t st = current_stream();
+    std::vector<uint64_t> levels{L};
+    while (levels.back() > kInverseCpuLimit) {
+        const uint64_t m = ((levels.back() - 2u) / 4u) & ~31ull;
+        levels.push_back(levels.back() - m * 2u);
+    }
+    const size_t L_res = (L + 31) / 32 + 2;
+    const size_t L_res2 = (L + 31) / 32 + 1;
+    const size_t L_y2 = x.length + 1;
+    TRY(ybuf.alloc(x.length));
+    y_out = BatchMPArray{ybuf.p, x.length, 1, x.length};
+    TRY(cudaMemsetAsync(ybuf.p, 0, (size_t)x.length * 4, st));
+    Buf ws;
+    TRY(ws.alloc(L_res + L_res2 + L_y2));
+    uint32_t *res_base = ws.p;
+    uint32_t *res2_base = ws.p + L_res;
+    uint32_t *y2_base = res2_base + L_res2;
+    TRY(cudaMemsetAsync(res_base, 0, L_res * 4, st));
+
+    BatchMPArray res;
+    {
+        const uint64_t L0 = levels.back();
+        const uint32_t start = (uint32_t)((L - L0) >> 6);
+        BatchMPArray x0 = subview(x, start, x.length - start);
+        BatchMPArray y0 = subview(y_out, start, y_out.length - start);
+        res = BatchMPArray{res_base + start * 2u, x0.length + 1u, 1, x0.length + 1u};
+        std::vector<uint32_t> hx(x0.length);
+        if (x0.length)
+            TRY(cudaMemcpyAsync(hx.data(), x0.data, (size_t)x0.length * 4, cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        std::vector<uint32_t> hq, hr;
+        divmod_pow2((uint32_t)L0, hx, hq, hr);
+        // store_mpz_to_device writes the whole stride (pi_bs_gpu.cu:1121-1141)
+        if (hq.size() > y0.stride || hr.size() > res.stride) return cudaErrorInvalidValue;
+        hq.resize(y0.stride, 0u);
+        hr.resize(res.stride, 0u);
+        TRY(cudaMemcpyAsync(y0.data, hq.data(), (size_t)y0.stride * 4, cudaMemcpyHostToDevice, st));
+        TRY(cudaMemcpyAsync(res.data, hr.data(), (size_t)res.stride * 4, cudaMemcpyHostToDevice, st));
+        TRY(cudaStreamSynchronize(st));
+    }
+    TRY(res.compact(ctx));
+
+    for (int i = (int)levels.size() - 1; i > 0; --i) {
+        const uint64_t L1 = levels[i], L2 = levels[i - 1];
+        const uint64_t m = (L2 - L1) >> 1;
+        const uint32_t dg = (uint32_t)(L2 >> 5);
+        BatchMPArray x2 = subview(x, (uint32_t)((L - L2) >> 6), (uint32_t)(m >> 5));
+        BatchMPArray y1 = subview(y_out, (uint32_t)((L - L1) >> 6), y_out.length - (uint32_t)((L - L1) >> 6));
+        BatchMPArray x2y1{res2_base, x2.length + y1.length, 1, x2.length + y1.length};
+        TRY(p_mul(ctx, pr, x2, y1, x2y1, "x2*y", dg));
+        BatchMPArray res1m{res.data - (uint32_t)(m >> 5), res.length + (uint32_t)(m >> 5) + 1u, 1,
+                           res.length + (uint32_t)(m >> 5) + 1u};
+        TRY(p_sub(ctx, pr, res1m, x2y1, res1m, "res1_m", dg));
+        uint32_t top = 0u;
+        TRY(cudaMemcpyAsync(&top, res1m.data + res1m.length - 1, 4, cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        const bool neg = top >= 0x80000000u;
+        if (neg) {
+            TRY(p_sub(ctx, pr, BatchMPArray{res1m.data, 0, 1, 0}, res1m, res1m, "res1_m_neg", dg));
+        }
+        BatchMPArray res2{res2_base, res1m.length + y1.length, 1, res1m.length + y1.length};
+        TRY(p_mul(ctx, pr, res1m, y1, res2, "res2*y", dg));
+        const uint32_t y2len = res2.length - (uint32_t)((L2 - m * 2) >> 5);
+        BatchMPArray y2{y2_base, y2len, 1, y2len};
+        TRY(shift_right_large(ctx, pr, res2, L2 - m * 2u, y2, "y2", dg));
+        if (neg) TRY(p_add_small(ctx, pr, y2, 1u, y2, "y2_inc", dg));
+        BatchMPArray ynew = subview(y_out, (uint32_t)((L - L2) >> 6), y_out.length - (uint32_t)((L - L2) >> 6));
+        if (!neg)
+            TRY(p_add(ctx, pr, ynew, y2, ynew, "(y<<m)+y2", dg));
+        else
+            TRY(p_sub(ctx, pr, ynew, y2, ynew, "(y<<m)-y2", dg));
+        if (L2 != L) {
+            BatchMPArray xn = subview(x, (uint32_t)((L - L2) >> 6), x.length - (uint32_t)((L - L2) >> 6));
+            res = BatchMPArray{res1m.data - (uint32_t)(m >> 5), res1m.length + (uint32_t)(m >> 5), 1,
+                               res1m.length + (uint32_t)(m >> 5)};
+            BatchMPArray y2x{res2_base, y2.length + xn.length, 1, y2.length + xn.length};
+            TRY(p_mul(ctx, pr, y2, xn, y2x, "y2*x", dg));
+            if (!neg)
+                TRY(p_sub(ctx, pr, res, y2x, res, "(res<<m)-y2x", dg));
+            else
+                TRY(p_sub(ctx, pr, y2x, res, res, "y2x-(res<<m)", dg));
+            TRY(res.compact(ctx));
+        }
+    }
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// pi_fractional (pi_bs_gpu.cu:1524-1685)
+// ---------------------------------------------------------------------------
+static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, Buf &retbuf, BatchMPArray &RET) {
+    cudaStream_t st = current_stream();
+    uint32_t N = 1;
+    while (N * 17 * 14.3 < target) N *= 2;
+    const int prec = (int)(((long)(target * 3.322) + 31) / 32 + 1);
+    Buf qbs, rbs;
+    BatchMPArray Qbs, Rbs;
+    TRY(binary_split(ctx, pr, N, qbs, Qbs, rbs, Rbs));
+    const long rts = 15l * N * 17 - 8;
+    const int rbits = (int)(rts % 32), rlimbs = (int)(rts / 32);
+    BatchMPArray Rpre{Rbs.data + rlimbs, Rbs.length - rlimbs, 1, Rbs.length - rlimbs};
+    Buf rsb;
+    TRY(rsb.alloc(Rpre.length + 1u));
+    BatchMPArray Rs{rsb.p, Rpre.length + 1u, 1, Rpre.length + 1u};
+    TRY(p_shift(ctx, pr, Rpre, Rs, -rbits, "R_shift", (uint32_t)target));
+    rbs.reset();
+    TRY(Rs.compact(ctx));
+    long extra = std::max(0l, std::min((long)Qbs.length, (long)Rs.length) - prec);
+    BatchMPArray Qt{Qbs.data + extra, Qbs.length - (uint32_t)extra, 1, Qbs.length - (uint32_t)extra};
+    BatchMPArray Rt{Rs.data + extra, Rs.length - (uint32_t)extra, 1, Rs.length - (uint32_t)extra};
+    Buf p15b, q15b;
+    BatchMPArray P15, Q15;
+    TRY(sqrt_10005(ctx, pr, target, p15b, P15, q15b, Q15));
+    Buf pfb, qfb;
+    BatchMPArray Pf{nullptr, P15.length + Qt.length, 1, P15.length + Qt.length};
+    BatchMPArray Qf{nullptr, Q15.length + Rt.length, 1, Q15.length + Rt.length};
+    TRY(pfb.alloc(Pf.stride));
+    TRY(qfb.alloc(Qf.stride));
+    Pf.data = pfb.p;
+    Qf.data = qfb.p;
+    TRY(p_mul(ctx, pr, P15, Qt, Pf, "P15*Q", (uint32_t)target));
+    TRY(p_mul(ctx, pr, Rt, Q15, Qf, "R*Q15", (uint32_t)target));
+    TRY(p_compact(ctx, pr, Pf, "P", (uint32_t)target));
+    TRY(p_compact(ctx, pr, Qf, "Q", (uint32_t)target));
+    qbs.reset();
+    rsb.reset();
+    p15b.reset();
+    q15b.reset();
+    extra = std::max(0l, std::min((long)Pf.length, (long)Qf.length) - prec);
+    BatchMPArray Ptf = subview(Pf, (uint32_t)extra, Pf.length - (uint32_t)extra);
+    BatchMPArray Qtf = subview(Qf, (uint32_t)extra, Qf.length - (uint32_t)extra);
+    TRY(Qtf.compact(ctx));
+    uint32_t qbits = 0u;
+    if (Qtf.length > 0u) {
+        uint32_t topl = 0u;
+        TRY(cudaMemcpyAsync(&topl, Qtf.data + Qtf.length - 1, 4, cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        qbits = (Qtf.length - 1u) * 32u + (topl ? 32u - (uint32_t)__builtin_clz(topl) : 0u);
+    }
+    const uint64_t inv_bits = (uint64_t)qbits * 2u - 1u;
+    Buf invb;
+    BatchMPArray inv;
+    TRY(recursive_inverse(ctx, pr, Qtf, inv_bits, invb, inv, (uint32_t)target));
+    qfb.reset();
+    Buf rpb;
+    BatchMPArray RP{nullptr, Ptf.length + inv.length, 1, Ptf.length + inv.length};
+    TRY(rpb.alloc(RP.stride));
+    RP.data = rpb.p;
+    TRY(p_mul(ctx, pr, Ptf, inv, RP, "P*invQ", (uint32_t)target));
+    TRY(p_compact(ctx, pr, RP, "P*invQ", (uint32_t)target));
+    pfb.reset();
+    invb.reset();
+    const uint32_t retlen = RP.length - (uint32_t)(inv_bits / 32u) + (uint32_t)prec;
+    TRY(retbuf.alloc(retlen));
+    RET = BatchMPArray{retbuf.p, retlen, 1, retlen};
+    const uint64_t fshift = inv_bits - (uint64_t)prec * 32u;
+    TRY(shift_right_large(ctx, pr, RP, fshift, RET, "RET_shift", (uint32_t)target));
+    TRY(p_compact(ctx, pr, RET, "RET", (uint32_t)target));
+    return cudaSuccess;
+}
+
+}  // namespace gpupi
+
+// ---------------------------------------------------------------------------
+// Public driver
+// ---------------------------------------------------------------------------
+namespace gpupi {
+
+uint32_t round_up_decimal_digits(uint32_t requested, uint32_t *leaf_out) {
+    // pi_bs_gpu.cu:924-939
+    if (requested == 0u) {
+        *leaf_out = 0u;
+        return 0u;
+    }
+    uint32_t digits = requested, levels = 0u;
+    while (digits >= 32u * 18u) {
+        digits >>= 1;
+        ++levels;
+    }
+    if ((digits << levels) < requested) ++digits;
+    *leaf_out = digits;
+    return digits << levels;
+}
+
+uint32_t prec_limbs_for_digits(uint32_t digits) {
+    const uint32_t bits = (uint32_t)((double)digits * 3.322) + 31u;   // pi_bs_gpu.cu:941-944
+    return bits / 32u + 1u;
+}
+
+cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
+    out = PiOutput{};
+    const uint32_t requested = req.digits;
+    uint32_t leaf = 0u;
+    const uint32_t convert = round_up_decimal_digits(requested, &leaf);
+    const uint32_t prec = prec_limbs_for_digits(requested);
+    out.target_digits = requested;
+    out.convert_digits = convert;
+    if (requested > 0u && convert == 0u) return cudaErrorInvalidValue;
+    BatchMPContext *ctx = req.ctx;
+    bool own_ctx = false;
+    if (!ctx) {
+        ctx = batch_mp_init();
+        own_ctx = true;
+        if (!ctx) return cudaErrorMemoryAllocation;
+    }
+    cudaStream_t st = current_stream();
+    Profiler prof;
+    prof.on = req.profile_stages;
+    const uint32_t levels = convert ? (uint32_t)__builtin_ctz(convert / leaf) : 0u;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaError_t err = cudaEventRecord(e0, st);
+    Buf retb;
+    BatchMPArray RET{};
+    ConvertDecimalPowerTable powers{};
+    char *d_digits = nullptr;
+    if (err == cudaSuccess) err = pi_fractional(ctx, &prof, (int)requested, retb, RET);
+    if (err == cudaSuccess) {
+        err = stage(&prof, "decimal_powers", "precompute_5pow", levels == 0u ? leaf : (leaf << levels), 1u, levels,
+                    leaf, false, [&]() { return convert_decimal_precompute_powers(ctx, &powers, leaf, levels); });
+    }
+    if (err == cudaSuccess && requested > 0u) {
+        err = cudaMallocAsync((void **)&d_digits, convert, st);
+        if (err == cudaSuccess) {
+            BatchMPArray frac = subview(RET, 0u, std::min<uint32_t>(prec, RET.length));
+            err = stage(&prof, "decimal_convert", "equal_split", convert, frac.batch_size, frac.length, leaf, false,
+                        [&]() {
+                            return convert_decimal_equal_split(ctx, frac, prec * 32u, convert, leaf, &powers,
+                                                               d_digits);
+                        });
+        }
+    }
+    if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&out.elapsed_ms, e0, e1);
+    out.ret_len = RET.length;
+    out.workspace_bytes = batch_mp_workspace_size(ctx);
+    if (err == cudaSuccess) {
+        out.ret.resize(RET.length);
+        if (RET.length)
+            err = cudaMemcpyAsync(out.ret.data(), RET.data, (size_t)RET.length * 4, cudaMemcpyDeviceToHost, st);
+        const uint32_t want = std::min(requested, req.copy_digits);
+        if (err == cudaSuccess && want > 0u) {
+            out.digits.resize(want);
+            err = cudaMemcpyAsync(&out.digits[0], d_digits, want, cudaMemcpyDeviceToHost, st);
+        }
+        if (err == cudaSuccess && req.copy_digits < requested && requested > 0u) {
+            // tail for the --benchmark preview
+            const uint32_t tail = std::min<uint32_t>(requested, 64u);
+            out.tail.resize(tail);
+            err = cudaMemcpyAsync(&out.tail[0], d_digits + (requested - tail), tail, cudaMemcpyDeviceToHost, st);
+        }
+        if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    }
+    out.stages = prof.entries;
+    if (d_digits) cudaFreeAsync(d_digits, st);
+    convert_decimal_release_powers(&powers);
+    retb.reset();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    if (own_ctx) batch_mp_destroy(ctx);
+    return err;
+}
+
+}  // namespace gpupi

@@ -1,0 +1,48 @@
+// Internal interface of the pi pipeline driver (pi_engine.cu).
+#pragma once
+
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "batch_arith.h"
+
+namespace gpupi {
+
+struct StageEntry {
+    const char *kind;
+    const char *label;
+    uint32_t n1, batch, lhs, rhs;
+    float ms;
+    bool uses_ntt;
+};
+
+struct PiRequest {
+    uint32_t digits = 0;            // requested decimal digits after the point
+    bool profile_stages = false;    // time every op (serialises the run)
+    uint32_t copy_digits = 0;       // how many leading digits to copy to the host
+    BatchMPContext *ctx = nullptr;  // reuse a context (keeps its workspace); null = private
+};
+
+struct PiOutput {
+    uint32_t target_digits = 0;
+    uint32_t convert_digits = 0;
+    uint32_t ret_len = 0;
+    float elapsed_ms = 0.f;
+    size_t workspace_bytes = 0;
+    std::vector<uint32_t> ret;      // RET limbs (little endian)
+    std::string digits;             // first copy_digits digits
+    std::string tail;               // last 64 requested digits when not all were copied
+    std::vector<StageEntry> stages;
+};
+
+cudaError_t pi_run(const PiRequest &req, PiOutput &out);
+uint32_t round_up_decimal_digits(uint32_t requested, uint32_t *leaf_out);
+uint32_t prec_limbs_for_digits(uint32_t digits);
+
+cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
+void set_school_max(uint32_t v);
+uint32_t school_max();
+
+}  // namespace gpupi

@@ -1,0 +1,174 @@
+// pi_bs_gpu command line (gpupi pi_bs_gpu.cu:2073-2437, main_fractional).
+//
+//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print]
+//
+// Same arguments, stdout/stderr lines and exit codes as the reference; the
+// computation is gpupi_b200's pipeline (pi_engine.cu).
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "pi_engine.h"
+
+namespace {
+
+constexpr uint32_t kValidationMod = 1000000007u;            // pi_bs_gpu.cu:149
+constexpr uint64_t kLimbBaseMod = (1ull << 32) % kValidationMod;
+
+bool parse_int_arg(const char *text, int *value) {
+    if (!text || !value) return false;
+    char *end = nullptr;
+    const long v = strtol(text, &end, 10);
+    if (end == text || *end != '\0') return false;
+    *value = (int)v;
+    return true;
+}
+
+uint32_t mod_hash(const uint32_t *limbs, uint32_t n) {           // pi_bs_gpu.cu:852-858
+    uint64_t v = 0;
+    for (int i = (int)n - 1; i >= 0; --i) v = (v * kLimbBaseMod + limbs[i]) % kValidationMod;
+    return (uint32_t)v;
+}
+
+uint32_t decimal_hash(const char *d, uint32_t n) {               // pi_bs_gpu.cu:860-866
+    uint64_t v = 3u;
+    for (uint32_t i = 0; i < n; ++i) v = (v * 10u + (uint32_t)(d[i] - '0')) % kValidationMod;
+    return (uint32_t)v;
+}
+
+void hex_preview(const char *label, const uint32_t *limbs, uint32_t length) {   // :868-896
+    const uint32_t hash = mod_hash(limbs, length);
+    if (length == 0) {
+        printf("%s = 0 hash = %u\n", label, hash);
+        return;
+    }
+    const uint32_t first = std::min(length, 2u), last = std::min(length, 2u);
+    printf("%s = ", label);
+    for (uint32_t i = 0; i < last; ++i) {
+        const uint32_t idx = length - 1 - i;
+        if (i == 0) printf("%x", limbs[idx]);
+        else printf("%08x", limbs[idx]);
+    }
+    if (length > first + last) printf("...");
+    for (uint32_t i = first; i > 0; --i) {
+        const uint32_t idx = i - 1;
+        if (length <= first + last && idx >= length - last) continue;
+        printf("%08x", limbs[idx]);
+    }
+    printf(" hash = %u\n", hash);
+}
+
+void usage(const char *prog) {
+    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print]\n", prog);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    int target = 0;
+    if (argc < 2 || !parse_int_arg(argv[1], &target) || target < 0) {
+        usage(argv[0]);
+        return 1;
+    }
+    const uint32_t requested = (uint32_t)target;
+    bool benchmark = false, profile = false, full = false;
+    if (argc >= 3) {
+        if (strcmp(argv[2], "--benchmark") == 0) benchmark = true;
+        else if (strcmp(argv[2], "--profile-stages") == 0) profile = true;
+        else if (strcmp(argv[2], "--full-print") == 0) full = true;
+        else {
+            usage(argv[0]);
+            return 1;
+        }
+    }
+    gpupi::PiRequest req;
+    req.digits = requested;
+    req.profile_stages = profile;
+    if (benchmark) req.copy_digits = std::min<uint32_t>(requested, 63u);
+    else if (profile) req.copy_digits = std::min<uint32_t>(requested, 4096u);
+    else req.copy_digits = requested;
+    gpupi::PiOutput out;
+    const cudaError_t err = gpupi::pi_run(req, out);
+    if (err != cudaSuccess) {
+        fprintf(stderr, "pi_fractional failed: %s\n", cudaGetErrorString(err));
+        return 1;
+    }
+    const int ws_mb = (int)(out.workspace_bytes / (1024 * 1024));
+    if (benchmark) {
+        printf("target_digits=%u convert_digits=%u RET_len=%u elapsed_ms=%.3f workspace_max=%dMB\n", requested,
+               out.convert_digits, out.ret_len, out.elapsed_ms, ws_mb);
+        hex_preview("RET", out.ret.data(), out.ret_len);
+        if (requested > 0u) {
+            const uint32_t suffix = std::min<uint32_t>(requested, 64u);
+            std::string tail = out.tail.empty() ? out.digits.substr(out.digits.size() - suffix) : out.tail;
+            printf("DEC = 3%s...%.*s\n", out.digits.c_str(), (int)suffix, tail.c_str());
+        } else {
+            printf("DEC = 3\n");
+        }
+        return 0;
+    }
+    if (profile) {
+        float leaf = 0, mul = 0, mul_small = 0, shift = 0, add = 0, sub = 0, compact = 0, exactdiv = 0,
+              dpow = 0, dconv = 0, ntt = 0;
+        for (size_t i = 0; i < out.stages.size(); ++i) {
+            const gpupi::StageEntry &e = out.stages[i];
+            if (!strcmp(e.kind, "leaf")) leaf += e.ms;
+            else if (!strcmp(e.kind, "mul")) {
+                mul += e.ms;
+                if (e.uses_ntt) ntt += e.ms;
+            } else if (!strcmp(e.kind, "mul_small")) mul_small += e.ms;
+            else if (!strcmp(e.kind, "shift")) shift += e.ms;
+            else if (!strcmp(e.kind, "add")) add += e.ms;
+            else if (!strcmp(e.kind, "sub")) sub += e.ms;
+            else if (!strcmp(e.kind, "compact")) compact += e.ms;
+            else if (!strcmp(e.kind, "exactdiv")) exactdiv += e.ms;
+            else if (!strcmp(e.kind, "decimal_powers")) dpow += e.ms;
+            else if (!strcmp(e.kind, "decimal_convert")) dconv += e.ms;
+            printf("stage[%03d] kind=%9s label=%18s digits=%8u batch=%8u lhs_len=%9u rhs_len=%9u kernel_ms=%6.3f "
+                   "uses_ntt=%d\n",
+                   (int)i, e.kind, e.label, e.n1, e.batch, e.lhs, e.rhs, e.ms, e.uses_ntt ? 1 : 0);
+        }
+        printf("leaf_total_ms=%.3f mul_total_ms=%.3f mul_small_total_ms=%.3f shift_total_ms=%.3f add_total_ms=%.3f "
+               "sub_total_ms=%.3f compact_total_ms=%.3f exactdiv_total_ms=%.3f decimal_powers_total_ms=%.3f "
+               "decimal_convert_total_ms=%.3f ntt_total_ms=%.3f\n",
+               leaf, mul, mul_small, shift, add, sub, compact, exactdiv, dpow, dconv, ntt);
+        const float acc = leaf + mul + mul_small + shift + add + sub + compact + exactdiv + dpow + dconv;
+        printf("target_digits=%u convert_digits=%u RET_len=%u elapsed_ms=%.3f accounted_ms=%.3f workspace_max=%dMB\n",
+               requested, out.convert_digits, out.ret_len, out.elapsed_ms, acc, ws_mb);
+        hex_preview("RET", out.ret.data(), out.ret_len);
+        if (requested > 0u)
+            printf("DEC_preview_hash = %u\n", decimal_hash(out.digits.data(), (uint32_t)out.digits.size()));
+        return 0;
+    }
+    fprintf(stderr, "target_digits=%u convert_digits=%u RET_len=%u elapsed_ms=%.3f\n", requested,
+            out.convert_digits, out.ret_len, out.elapsed_ms);
+    if (full) {
+        printf("RET = ");
+        if (out.ret_len == 0) {
+            printf("0\n");
+        } else {
+            for (int i = (int)out.ret_len - 1; i >= 0; --i) {
+                if (i == (int)out.ret_len - 1) printf("%x", out.ret[i]);
+                else printf("%08x", out.ret[i]);
+            }
+            printf("\n");
+        }
+        if (requested == 0u) {
+            printf("DEC = 3\n");
+        } else {
+            printf("DEC = 3");
+            fwrite(out.digits.data(), 1, requested, stdout);
+            printf("\n");
+        }
+    } else {
+        fputc('3', stdout);
+        if (requested > 0u) fwrite(out.digits.data(), 1, requested, stdout);
+    }
+    fputc('\n', stdout);
+    return 0;
+}

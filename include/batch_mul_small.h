@@ -1,0 +1,9 @@
+// C = A * B for a single host limb B over L_a + 1 limbs, truncated or
+// zero-extended to L_c (drop-in for gpupi batch_mul_small.h:6-35).
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+void batch_mul_small(const uint32_t *A, uint32_t B, uint32_t *C, uint32_t *workspace, uint32_t N,
+                     uint32_t L_a, uint32_t L_c, uint32_t stride_A, uint32_t stride_C);
+size_t batch_mul_small_workspace_size(uint32_t N, uint32_t L_a, uint32_t L_c);

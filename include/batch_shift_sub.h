@@ -1,0 +1,11 @@
+// C = (A << shift) - B modulo 2^(32*L_c); C must not alias A or B
+// (drop-in for gpupi batch_shift_sub.h:6-40).
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+void batch_shift_sub_simple(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t *workspace,
+                            uint32_t shift, uint32_t N, uint32_t L_a, uint32_t L_b, uint32_t L_c,
+                            uint32_t stride_A, uint32_t stride_B, uint32_t stride_C);
+size_t batch_shift_sub_simple_workspace_size(uint32_t N, uint32_t L_a, uint32_t L_b, uint32_t L_c,
+                                             uint32_t shift);

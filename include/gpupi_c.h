@@ -1,0 +1,108 @@
+/* C ABI of gpupi_b200 (libgpupi_b200.so).
+ *
+ * Plain pointers and sizes only.  Every pointer named d_* is device memory;
+ * h_* is host memory.  Functions return a cudaError_t value as int (0 =
+ * success, 1 = cudaErrorInvalidValue for malformed arguments, 2 = allocation
+ * failure).  Work is queued on the library's current stream
+ * (gpupi_set_stream), the legacy default stream unless changed.
+ *
+ * Each batched entry point mirrors one gpupi function; the reference
+ * declaration it replaces is cited beside it.  A batch item i of an operand X
+ * lives at d_X + i*stride_X (stride 0 broadcasts item 0), exactly like
+ * gpupi's BatchMPArray (batch_arith.h:10-22).
+ */
+#ifndef GPUPI_C_H
+#define GPUPI_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gpupi_ctx gpupi_ctx; /* wraps BatchMPContext */
+
+/* Library identification and launch accounting. */
+const char *gpupi_version(void);
+uint64_t gpupi_launch_count(void);
+int gpupi_set_stream(void *cuda_stream);
+int gpupi_device_sync(void);
+
+/* batch_mp_init / batch_mp_destroy / batch_mp_workspace_size /
+ * batch_mp_ensure_workspace (batch_arith.h:35-43) */
+gpupi_ctx *gpupi_ctx_create(void);
+void gpupi_ctx_destroy(gpupi_ctx *ctx);
+size_t gpupi_ctx_workspace_size(const gpupi_ctx *ctx);
+int gpupi_ctx_ensure_workspace(gpupi_ctx *ctx, size_t bytes);
+
+/* batch_mp_mul (batch_arith.h:48-53): C = A * B, L_c must be L_a + L_b. */
+int gpupi_mp_mul(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                 const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t L_c,
+                 uint32_t stride_C);
+/* batch_mp_add / batch_mp_sub (batch_arith.h:75-80, 115-120) */
+int gpupi_mp_add(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                 const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t L_c,
+                 uint32_t stride_C);
+int gpupi_mp_sub(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                 const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t L_c,
+                 uint32_t stride_C);
+/* batch_mp_shift_add / batch_mp_shift_sub (batch_arith.h:94-111) */
+int gpupi_mp_shift_add(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                       const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t shift, uint32_t *d_C,
+                       uint32_t L_c, uint32_t stride_C);
+int gpupi_mp_shift_sub(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                       const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t shift, uint32_t *d_C,
+                       uint32_t L_c, uint32_t stride_C);
+/* batch_mp_add_small / sub_small / mul_small (batch_arith.h:57-62, 84-89, 124-129) */
+int gpupi_mp_add_small(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                       uint32_t b, uint32_t *d_C, uint32_t L_c, uint32_t stride_C);
+int gpupi_mp_sub_small(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                       uint32_t b, uint32_t *d_C, uint32_t L_c, uint32_t stride_C);
+int gpupi_mp_mul_small(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                       uint32_t b, uint32_t *d_C, uint32_t L_c, uint32_t stride_C);
+/* batch_mp_exactdiv_small (batch_arith.h:67-71): in place, b odd, L_a <= 128 */
+int gpupi_mp_exactdiv_small(gpupi_ctx *ctx, uint32_t N, uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                            uint32_t b);
+/* batch_mp_shift_bits (batch_arith.h:132-137) */
+int gpupi_mp_shift_bits(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                        uint32_t *d_B, uint32_t L_b, uint32_t stride_B, int32_t shift_bits);
+/* batch_mp_bitlength_max / batch_mp_limblength_max (batch_arith.h:140-151) */
+int gpupi_mp_bitlength_max(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                           uint32_t *h_result);
+int gpupi_mp_limblength_max(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                            uint32_t *h_result);
+
+/* batch_mul_naive (batch_mul_naive.h:16-25) and batch_mul_ntt
+ * (batch_mul_ntt.h:24-40) called directly, bypassing the crossover. */
+int gpupi_mul_naive(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A, const uint32_t *d_B,
+                    uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t stride_C);
+int gpupi_mul_ntt(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                  const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t stride_C);
+
+/* batch_decimal_naive (batch_decimal_naive.h:23-31): LSD-first ASCII digits */
+int gpupi_decimal_naive(uint32_t N, const uint32_t *d_A, uint32_t L_limb, uint32_t stride_A, char *d_out,
+                        uint32_t L_dec, uint32_t stride_out);
+/* convert_decimal_precompute_powers + convert_decimal_equal_split
+ * (convert_decimal.h:16-41) in one call; d_out gets total_digits digits in
+ * natural order. */
+int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *d_X, uint32_t L_x, uint32_t input_bits,
+                          uint32_t total_digits, uint32_t leaf_digits, char *d_out);
+
+/* Whole pi_bs_gpu pipeline (pi_bs_gpu.cu:2073-2431, main_fractional).
+ * h_ret (capacity ret_cap limbs) receives RET, h_digits (capacity digits_cap)
+ * the first min(digits, digits_cap) decimal digits after "3.".  Either may be
+ * null.  info[0..7] receives: convert_digits, RET length, elapsed ms on the
+ * device (float bits), workspace MB, number of profiled stages, leaf digits,
+ * 0, 0.  flags bit 0 = profile every stage. */
+int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
+                     char *h_digits, size_t digits_cap, uint32_t *info);
+
+/* Multiply crossover: largest L_a + L_b computed by schoolbook (<= 1024). */
+int gpupi_set_mul_crossover(uint32_t max_school_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

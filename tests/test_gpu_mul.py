@@ -1,0 +1,105 @@
+"""Parity of the batched multiply (schoolbook tiers, three-prime NTT with one,
+two and three passes, broadcast and squaring) against exact Python integers.
+
+Mirrors batch_mul_ntt_test.cu (random strides with padding :289-293, size
+sweeps :373-402, large-L cases :543-556) and batch_arith_test.cu's crossover
+cases (:98-102).  Bit-exact.
+"""
+import numpy as np
+import pytest
+
+import batch_ref as ref
+from helpers import rand_buf, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_mul(ctx, N, La, Lb, sA, sB, sC, rng, path="auto", extreme=False):
+    A, B, C = rand_buf(rng, N, sA, La), rand_buf(rng, N, sB, Lb), rand_buf(rng, N, sC, 0)
+    if extreme:   # all-ones operands: largest coefficients and longest carries
+        for r in range(N):
+            A[r * sA: r * sA + La] = 0xFFFFFFFF
+            B[r * sB: r * sB + Lb] = 0xFFFFFFFF
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    if path == "ntt":
+        ctx.mul_ntt(N, dA.ptr, La, sA, dB.ptr, Lb, sB, dC.ptr, sC)
+    elif path == "naive":
+        import gpupi_b200 as g
+        g.mul_naive(N, dA.ptr, La, sA, dB.ptr, Lb, sB, dC.ptr, sC)
+    else:
+        ctx.mul(N, dA.ptr, La, sA, dB.ptr, Lb, sB, dC.ptr, La + Lb, sC)
+    got = dC.numpy()
+    if La + Lb <= 300000:
+        assert np.array_equal(got, ref.mul(N, A, La, sA, B, Lb, sB, C, sC))
+    else:
+        # too large for an exact Python product: residues mod 4 primes + exact low limbs
+        assert ref.mul_check(N, A, La, sA, B, Lb, sB, got, sC)
+
+
+@pytest.mark.parametrize("La,Lb", [(1, 1), (3, 3), (4, 3), (6, 4), (8, 8), (12, 5), (16, 16), (17, 16),
+                                   (33, 31), (100, 7), (256, 256), (511, 513), (1000, 24)])
+def test_schoolbook(ctx, La, Lb):
+    rng = np.random.default_rng(La * 1000 + Lb)
+    N = 300 if La + Lb < 64 else 17
+    _check_mul(ctx, N, La, Lb, La + 3, Lb + 1, La + Lb + 2, rng, path="naive")
+    _check_mul(ctx, 3, La, Lb, La, Lb, La + Lb, rng, path="naive", extreme=True)
+
+
+@pytest.mark.parametrize("La,Lb", [(1, 1), (2, 3), (100, 100), (513, 511), (1000, 1000), (2048, 2048),
+                                   (3000, 1097), (2049, 2048)])
+def test_ntt_single_pass(ctx, La, Lb):
+    rng = np.random.default_rng(100 + La + Lb)
+    _check_mul(ctx, 5, La, Lb, La + 1, Lb + 2, La + Lb + 3, rng, path="ntt")
+    _check_mul(ctx, 2, La, Lb, La, Lb, La + Lb, rng, path="ntt", extreme=True)
+
+
+@pytest.mark.parametrize("La,Lb,N", [(4097, 1, 2), (4096, 4097, 3), (20000, 30000, 2), (100000, 70000, 1),
+                                     (1 << 20, 1 << 20, 1)])
+def test_ntt_two_pass(ctx, La, Lb, N):
+    rng = np.random.default_rng(La ^ Lb)
+    _check_mul(ctx, N, La, Lb, La, Lb, La + Lb, rng, path="ntt")
+
+
+def test_ntt_extreme_coefficients(ctx):
+    """All-ones operands make every convolution coefficient maximal."""
+    rng = np.random.default_rng(0)
+    _check_mul(ctx, 1, 150000, 150000, 150000, 150000, 300000, rng, path="ntt", extreme=True)
+    _check_mul(ctx, 1, 1 << 21, 1 << 21, 1 << 21, 1 << 21, 1 << 22, rng, path="ntt", extreme=True)
+
+
+def test_ntt_three_pass(ctx):
+    """K = 2^23 points: two column passes + the row pass."""
+    rng = np.random.default_rng(2 ** 22)
+    _check_mul(ctx, 1, 3_000_000, 2_500_000, 3_000_000, 2_500_000, 5_500_000, rng, path="ntt")
+
+
+def test_broadcast_and_square(ctx):
+    """stride 0 broadcast of B (convert_decimal.cu:401-406) and A*A."""
+    rng = np.random.default_rng(77)
+    N, La, Lb = 9, 6000, 5000
+    A, B, C = rand_buf(rng, N, La, La), rand_buf(rng, 1, Lb, Lb), rand_buf(rng, N, La + Lb, 0)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    ctx.mul(N, dA.ptr, La, La, dB.ptr, Lb, 0, dC.ptr, La + Lb, La + Lb)
+    assert np.array_equal(dC.numpy(), ref.mul(N, A, La, La, B, Lb, 0, C, La + Lb))
+    S = rand_buf(rng, 1, 2 * La, 0)
+    dS = to_dev(S)
+    ctx.mul(1, dA.ptr, La, La, dA.ptr, La, La, dS.ptr, 2 * La, 2 * La)
+    assert np.array_equal(dS.numpy(), ref.mul(1, A, La, La, A, La, La, S, 2 * La))
+
+
+@pytest.mark.parametrize("L", [510, 511, 512, 513, 1023, 1024, 1025])
+def test_crossover_boundary(ctx, L):
+    """Products on both sides of the schoolbook/NTT crossover (batch_arith_test.cu:98-102)."""
+    rng = np.random.default_rng(L)
+    _check_mul(ctx, 4, L // 2, L - L // 2, L // 2, L - L // 2, L, rng)
+
+
+def test_uneven_pairs_sample(ctx):
+    """A sample of the 4096-uneven-pairs workload: log-uniform lengths in
+    [8, 4096] per operand, one call per pair (the reference API takes a single
+    length per batch)."""
+    rng = np.random.default_rng(0xC2)
+    for _ in range(24):
+        La = int(2 ** rng.uniform(3, 12))
+        Lb = int(2 ** rng.uniform(3, 12))
+        _check_mul(ctx, 1, La, Lb, La, Lb, La + Lb, rng)

@@ -1,0 +1,38 @@
+"""End-to-end parity of the pi pipeline (pi_bs_gpu main_fractional) against
+the CPU restatement (RET limbs and every digit) and the committed golden
+fixtures (RET hash / length, digit hashes) up to 1e6 digits."""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import pi_ref
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "pi_golden.json").read_text())
+
+
+@pytest.mark.parametrize("digits", [0, 1, 10, 100, 575, 576, 1000, 5000, 20000, 100000])
+def test_pi_matches_oracle(ctx, digits):
+    import gpupi_b200 as g
+    r = g.pi_compute(digits, ctx)
+    want = pi_ref.pi_digits(digits)
+    assert r.ret_len == want.ret_len
+    assert np.array_equal(r.ret, np.array(pi_ref.to_limbs(want.ret, want.ret_len), dtype=np.uint32))
+    assert r.convert_digits == want.convert_digits
+    assert r.dec == want.digits[:digits]
+
+
+@pytest.mark.parametrize("entry", GOLDEN["runs"], ids=lambda e: str(e["digits"]))
+def test_pi_golden(ctx, entry):
+    import gpupi_b200 as g
+    d = entry["digits"]
+    r = g.pi_compute(d, ctx)
+    assert r.ret_len == entry["ret_len"]
+    assert pi_ref.mod_hash(r.ret) == entry["ret_hash"]
+    assert r.convert_digits == entry["convert_digits"]
+    assert hashlib.sha256(r.dec.encode()).hexdigest() == entry["dec_sha256"]
+    assert pi_ref.decimal_hash(r.dec[:4096]) == entry["dec_preview_hash"]
