@@ -1,0 +1,290 @@
+#!/usr/bin/env python
+"""Benchmark: milliseconds to compute pi to 1,000,000,000 decimal digits on a
+B200 with gpupi_b200 (the pi_bs_gpu pipeline: Chudnovsky binary splitting,
+Pell sqrt(10005), recursive reciprocal, final product, decimal conversion).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--digits D]
+
+One JSON line on stdout (rank 0).  A step is one full pipeline run.  The
+pipeline does not shard (it is one dependent chain of products), so N > 1
+runs N independent replicas, one per GPU, timed as the max over ranks.
+
+Our arm (``--impl ours``):
+  value      device time per step (CUDA events on the library's stream), RET
+             and digits left in HBM (no host copies inside the step);
+  e2e        the same computation through the C ABI call with the digits and
+             RET copied into pinned host memory every step (wall clock);
+  roofline   the kernel family with the largest share of device time, its
+             algorithmic bytes / its event-timed duration, against the
+             measured HBM copy bandwidth;
+  cpu_baseline  the CPU restatement (oracle) on a bounded sample, rank 0.
+The reference arm (``--impl reference``) times the CPU restatement of the
+same pipeline (the reference ships no CPU implementation) on a bounded
+sample per step, extrapolated linearly to the metric's digit count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ms to 1e9 digits of pi (bit-exact), tuned vs plain form on B200; NTT HBM GB/s"
+CPU_SAMPLE_DIGITS = 1_000_000          # ~18 s on one host core
+REF_SAMPLE_DIGITS = 200_000            # per reference-arm step, ~1.5 s
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = Path(f"/tmp/gpupi_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        loaded = [s for s in sm if s > 0.5 * max(smax or [1])] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline_sample(digits: int) -> dict:
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pi_ref
+    t0 = time.perf_counter()
+    pi_ref.pi_digits(digits)
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"value": ms * (1e9 / digits), "unit": "ms (linear extrapolation to 1e9 digits)", "cores": 1,
+            "kind": "port",
+            "sample": f"pi to {digits} digits with the CPU restatement of the pipeline (oracle/pi_ref.py, "
+                      f"CPython big integers, one core): {ms:.1f} ms, scaled by 1e9/{digits} "
+                      f"(a lower bound: binary splitting grows faster than linearly)",
+            "sample_ms": ms}
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pi_ref
+    d = REF_SAMPLE_DIGITS
+    for _ in range(args.warmup):
+        pi_ref.pi_digits(d)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        pi_ref.pi_digits(d)
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.mean(times) * (args.digits / d)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (pi has no input data)",
+        "config": {"workload": f"pi to {args.digits} digits", "sample_digits_per_step": d,
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
+                         "sample": f"pi to {d} digits per step with oracle/pi_ref.py (the reference has no CPU "
+                                   f"implementation), mean of {args.steps} steps scaled linearly to {args.digits}"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import gpupi_b200 as g
+
+    torch.cuda.set_device(local)
+    ctx = g.Context()
+    digits = args.digits
+    # warm-up (also sizes the workspace and the stream-ordered pool)
+    for _ in range(args.warmup):
+        g.pi_compute(digits, ctx, device_only=True)
+    torch.cuda.synchronize()
+
+    # device-timed steps, results stay in HBM; kernel timers on for the roofline
+    g.timer_reset()
+    g.timer_enable(True)
+    clocks = Clocks(local)
+    _barrier(ws)
+    torch.cuda.synchronize()
+    launches0 = g.launch_count()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    inner = []
+    for _ in range(args.steps):
+        r = g.pi_compute(digits, ctx, device_only=True)
+        inner.append(r.elapsed_ms)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    _barrier(ws)
+    launches = g.launch_count() - launches0
+    g.timer_enable(False)
+    ktimes = g.timer_report()
+    ms_local = e0.elapsed_time(e1) / args.steps
+    ms = _max_over_ranks(ms_local, ws)
+
+    # end to end through the C ABI, digits + RET copied to pinned host memory
+    pinned = torch.empty(digits, dtype=torch.uint8, pin_memory=True)
+    h0, d0 = g.transfer_bytes()
+    e2e_times = []
+    ret_hash = None
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = g.pi_compute(digits, ctx, host_digits=pinned)
+        torch.cuda.synchronize()
+        e2e_times.append((time.perf_counter() - t0) * 1e3)
+    h1, d1 = g.transfer_bytes()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    head = bytes(pinned[:50].numpy()).decode()
+    if head != "14159265358979323846264338327950288419716939937510"[:min(50, digits)]:
+        raise SystemExit(f"bench: digits do not start like pi: {head}")
+    from pi_ref import mod_hash
+    ret_hash = mod_hash(r.ret)
+    e2e = _max_over_ranks(statistics.mean(e2e_times), ws)
+
+    # roofline of the dominant kernel family
+    peaks = _peaks()
+    dom = max(ktimes.items(), key=lambda kv: kv[1][1]) if ktimes else None
+    total_kernel_ms = sum(v[1] for v in ktimes.values())
+    roof = None
+    if dom:
+        name, (n, kms, kbytes) = dom
+        achieved = kbytes / (kms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "launches_per_step": n / args.steps, "share_of_kernel_time": kms / total_kernel_ms,
+                "peak_source": "measured" if not peaks.get("fallback") else "fallback"}
+    families = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
+                    "GBps": (v[2] / (v[1] * 1e-3) / 1e9) if v[1] > 0 else None} for k, v in ktimes.items()}
+
+    if rank != 0:
+        return
+    cpu = cpu_baseline_sample(CPU_SAMPLE_DIGITS) if (ws == 1 and not args.no_cpu) else None
+    line = {
+        "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (pi has no input data)",
+        "config": {"workload": f"pi to {digits} decimal digits (pi_bs_gpu {digits})", "digits": digits,
+                   "form": "plain (one op per launch, compact after every op, reference op sequence)",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                   "l2": "working set (tens of GB) larger than L2; no flush needed"},
+        "pipeline_elapsed_ms": statistics.mean(inner),
+        "ret_len": r.ret_len, "ret_hash": ret_hash, "convert_digits": r.convert_digits,
+        "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": (h1 - h0) // args.steps,
+                "d2h_bytes_per_step": (d1 - d0) // args.steps},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "kernel_families": families,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--digits", type=int, default=1_000_000_000)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    ws, rank, local = _dist()
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -57,6 +57,10 @@ _SIGS = [
     ("gpupi_convert_decimal", ctypes.c_int, [_p, _p, _u32, _u32, _u32, _u32, _p]),
     ("gpupi_pi_compute", ctypes.c_int,
      [_p, _u32, _u32, _p, ctypes.c_size_t, _p, ctypes.c_size_t, ctypes.POINTER(_u32)]),
+    ("gpupi_timer_enable", ctypes.c_int, [ctypes.c_int]),
+    ("gpupi_timer_reset", ctypes.c_int, []),
+    ("gpupi_timer_report", ctypes.c_size_t, [_p, ctypes.c_size_t]),
+    ("gpupi_transfer_bytes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
 ]
 
@@ -231,6 +235,33 @@ def launch_count() -> int:
     return int(lib().gpupi_launch_count())
 
 
+def timer_enable(on: bool) -> None:
+    lib().gpupi_timer_enable(1 if on else 0)
+
+
+def timer_reset() -> None:
+    lib().gpupi_timer_reset()
+
+
+def timer_report() -> dict:
+    """{kernel family: (launches, total_ms, total_algorithmic_bytes)}"""
+    l = lib()
+    n = l.gpupi_timer_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    l.gpupi_timer_report(buf, n + 1)
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms, by = line.split()
+        out[name] = (int(cnt), float(ms), float(by))
+    return out
+
+
+def transfer_bytes() -> tuple[int, int]:
+    h, d = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    lib().gpupi_transfer_bytes(ctypes.byref(h), ctypes.byref(d))
+    return h.value, d.value
+
+
 def set_mul_crossover(v: int) -> None:
     _check(lib().gpupi_set_mul_crossover(v), "gpupi_set_mul_crossover")
 
@@ -251,21 +282,33 @@ class PiResult:
 
 
 def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None = None,
-               ret_capacity: int | None = None) -> PiResult:
-    """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional)."""
+               ret_capacity: int | None = None, device_only: bool = False, profile: bool = False,
+               host_digits=None) -> PiResult:
+    """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional).
+
+    ``host_digits``: optional writable host buffer (e.g. a pinned torch uint8
+    tensor) receiving the digits directly from the device.  ``device_only``
+    keeps RET and the digits on the device (no host copies at all)."""
     _torch()
     l = lib()
     if copy_digits is None:
-        copy_digits = digits
+        copy_digits = 0 if device_only else digits
     if ret_capacity is None:
-        ret_capacity = (int(digits * 3.322) + 31) // 32 + 8
+        ret_capacity = 0 if device_only else (int(digits * 3.322) + 31) // 32 + 8
     ret = np.zeros(max(ret_capacity, 1), dtype=np.uint32)
-    dec = ctypes.create_string_buffer(max(copy_digits, 1))
+    if host_digits is not None:
+        dptr = host_digits.data_ptr() if hasattr(host_digits, "data_ptr") else ctypes.addressof(host_digits)
+        dbuf = None
+    else:
+        dbuf = ctypes.create_string_buffer(max(copy_digits, 1))
+        dptr = ctypes.addressof(dbuf) if copy_digits else None
     info = (_u32 * 8)()
-    rc = l.gpupi_pi_compute(ctx.h if ctx else None, digits, 0, ret.ctypes.data, ret.size,
-                            ctypes.addressof(dec) if copy_digits else None, copy_digits, info)
+    flags = (1 if profile else 0) | (2 if device_only else 0)
+    rc = l.gpupi_pi_compute(ctx.h if ctx else None, digits, flags, ret.ctypes.data if ret_capacity else None,
+                            ret_capacity, dptr, copy_digits, info)
     _check(rc, "gpupi_pi_compute")
     ret_len = info[1]
     elapsed = np.frombuffer(np.uint32(info[2]).tobytes(), dtype=np.float32)[0]
-    return PiResult(digits, info[0], ret_len, float(elapsed), info[3], ret[:ret_len].copy(),
-                    dec.raw[:copy_digits].decode("ascii"), info[5])
+    dec = dbuf.raw[:copy_digits].decode("ascii") if dbuf is not None else ""
+    return PiResult(digits, info[0], ret_len, float(elapsed), info[3],
+                    ret[:ret_len].copy() if ret_capacity else None, dec, info[5])

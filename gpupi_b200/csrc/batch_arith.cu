@@ -20,8 +20,14 @@
 #include "batch_sub.h"
 #include "batch_sub_small.h"
 
+#include <string.h>
+
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <new>
+#include <string>
+#include <vector>
 
 namespace gpupi {
 
@@ -32,6 +38,97 @@ cudaStream_t current_stream() { return g_stream; }
 void set_current_stream(cudaStream_t s) { g_stream = s; }
 uint64_t launch_counter() { return g_launches.load(); }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+static std::atomic<uint64_t> g_h2d{0}, g_d2h{0};
+void note_h2d(uint64_t b) { g_h2d.fetch_add(b, std::memory_order_relaxed); }
+void note_d2h(uint64_t b) { g_d2h.fetch_add(b, std::memory_order_relaxed); }
+void transfer_bytes(uint64_t *h2d, uint64_t *d2h) {
+    if (h2d) *h2d = g_h2d.load();
+    if (d2h) *d2h = g_d2h.load();
+}
+
+namespace {
+struct TimerRec {
+    const char *name;
+    cudaEvent_t a, b;
+    double bytes;
+};
+struct TimerState {
+    std::mutex mu;
+    bool on = false;
+    std::vector<TimerRec> recs;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+};
+TimerState &timer() {
+    static TimerState t;
+    return t;
+}
+cudaEvent_t pool_event(TimerState &t) {
+    if (t.used == t.pool.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        t.pool.push_back(e);
+    }
+    return t.pool[t.used++];
+}
+}  // namespace
+
+bool kernel_timer_enabled() { return timer().on; }
+void kernel_timer_enable(bool on) { timer().on = on; }
+void kernel_timer_reset() {
+    TimerState &t = timer();
+    std::lock_guard<std::mutex> g(t.mu);
+    t.recs.clear();
+    t.used = 0;
+}
+int kernel_timer_begin(const char *name) {
+    TimerState &t = timer();
+    if (!t.on) return -1;
+    std::lock_guard<std::mutex> g(t.mu);
+    TimerRec r{name, pool_event(t), pool_event(t), 0.0};
+    cudaEventRecord(r.a, g_stream);
+    t.recs.push_back(r);
+    return (int)t.recs.size() - 1;
+}
+void kernel_timer_end(int slot, double bytes) {
+    if (slot < 0) return;
+    TimerState &t = timer();
+    std::lock_guard<std::mutex> g(t.mu);
+    cudaEventRecord(t.recs[slot].b, g_stream);
+    t.recs[slot].bytes = bytes;
+}
+size_t kernel_timer_report(char *buf, size_t cap) {
+    TimerState &t = timer();
+    std::lock_guard<std::mutex> g(t.mu);
+    cudaDeviceSynchronize();
+    struct Agg {
+        uint64_t n = 0;
+        double ms = 0, bytes = 0;
+    };
+    std::map<std::string, Agg> agg;
+    for (const TimerRec &r : t.recs) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        Agg &x = agg[r.name];
+        x.n++;
+        x.ms += ms;
+        x.bytes += r.bytes;
+    }
+    std::string out;
+    char line[256];
+    for (auto &kv : agg) {
+        snprintf(line, sizeof(line), "%s %llu %.6f %.0f\n", kv.first.c_str(), (unsigned long long)kv.second.n,
+                 kv.second.ms, kv.second.bytes);
+        out += line;
+    }
+    if (buf && cap) {
+        const size_t n = std::min(cap - 1, out.size());
+        memcpy(buf, out.data(), n);
+        buf[n] = 0;
+    }
+    return out.size();
+}
 
 void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La,
                 uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC);

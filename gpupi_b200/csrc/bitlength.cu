@@ -51,6 +51,7 @@ static uint32_t length_max(const uint32_t *A, uint32_t *workspace, uint32_t N, u
     GPUPI_LAUNCH_CHECK();
     uint32_t h = 0u;
     cudaMemcpyAsync(&h, workspace, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    note_d2h(sizeof(uint32_t));
     cudaStreamSynchronize(st);
     return h;
 }

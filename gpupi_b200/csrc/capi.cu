@@ -161,6 +161,8 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
     req.profile_stages = (flags & 1u) != 0u;
     req.copy_digits = h_digits ? (uint32_t)std::min<size_t>(digits_cap, digits) : 0u;
     req.ctx = raw(ctx);
+    req.device_only = (flags & 2u) != 0u;
+    req.host_digits = h_digits;
     gpupi::PiOutput out;
     cudaError_t err = gpupi::pi_run(req, out);
     if (err != cudaSuccess) return (int)err;
@@ -168,7 +170,6 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
         const size_t n = std::min<size_t>(ret_cap, out.ret.size());
         memcpy(h_ret, out.ret.data(), n * 4);
     }
-    if (h_digits && !out.digits.empty()) memcpy(h_digits, out.digits.data(), out.digits.size());
     if (info) {
         uint32_t leaf = 0u;
         gpupi::round_up_decimal_digits(digits, &leaf);
@@ -181,6 +182,23 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
         info[6] = 0u;
         info[7] = 0u;
     }
+    return 0;
+}
+
+int gpupi_timer_enable(int on) {
+    gpupi::kernel_timer_enable(on != 0);
+    return 0;
+}
+
+int gpupi_timer_reset(void) {
+    gpupi::kernel_timer_reset();
+    return 0;
+}
+
+size_t gpupi_timer_report(char *buf, size_t cap) { return gpupi::kernel_timer_report(buf, cap); }
+
+int gpupi_transfer_bytes(uint64_t *h2d, uint64_t *d2h) {
+    gpupi::transfer_bytes(h2d, d2h);
     return 0;
 }
 

@@ -51,6 +51,7 @@ struct GenTwo {
         x = (j < La) ? A[row * sA + j] : 0u;
         y = (j < Lb) ? B[row * sB + j] : 0u;
     }
+    double read_limbs(uint32_t Lc) const { return (double)std::min(La, Lc) + std::min(Lb, Lc); }
 };
 
 struct GenSmall {
@@ -63,6 +64,7 @@ struct GenSmall {
         x = (j < La) ? A[row * sA + j] : 0u;
         y = (j == 0u) ? b : 0u;
     }
+    double read_limbs(uint32_t Lc) const { return (double)std::min(La, Lc); }
 };
 
 struct GenMulSmall {
@@ -76,6 +78,7 @@ struct GenMulSmall {
         x = (j < La) ? r[j] * b : 0u;
         y = (j >= 1u && j - 1u < La) ? __umulhi(r[j - 1u], b) : 0u;
     }
+    double read_limbs(uint32_t Lc) const { return (double)std::min(La, Lc); }
 };
 
 struct GenShiftTwo {
@@ -96,6 +99,7 @@ struct GenShiftTwo {
         x = (bit == 0u) ? lo : ((lo << bit) | (prev >> (32u - bit)));
         y = (j < Lb) ? B[row * sB + j] : 0u;
     }
+    double read_limbs(uint32_t Lc) const { return (double)std::min(La, Lc) + std::min(Lb, Lc); }
 };
 
 // ---------------------------------------------------------------------------
@@ -271,6 +275,7 @@ static void run_carry(const Gen &gen, uint32_t *C, uint32_t N, uint32_t Lc, uint
     if (N == 0u || Lc == 0u) return;
     cudaStream_t st = current_stream();
     const CarryPlan plan = plan_for(N, Lc);
+    KernelTimed kt("carry_chain", 4.0 * N * (gen.read_limbs(Lc) + (double)Lc));
     if (plan == CarryPlan::Thread) {
         carry_thread_rows<Gen, SUB><<<grid_for(N, 128), 128, 0, st>>>(gen, C, sC, N, Lc);
         GPUPI_LAUNCH_CHECK();

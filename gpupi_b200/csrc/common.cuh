@@ -33,6 +33,30 @@ void set_current_stream(cudaStream_t s);
 uint64_t launch_counter();
 void count_launch();
 
+// Host<->device bytes moved by this library (pipeline inputs/results,
+// compact() results, base-case round trips).
+void note_h2d(uint64_t bytes);
+void note_d2h(uint64_t bytes);
+void transfer_bytes(uint64_t *h2d, uint64_t *d2h);
+
+// Optional per-kernel timing: when enabled, the launch sites bracket each
+// launch with CUDA events on the current stream and record the launch's
+// algorithmic HBM bytes.  Resolved (after a synchronisation) by
+// kernel_timer_report().  Off by default: no events are recorded.
+bool kernel_timer_enabled();
+void kernel_timer_enable(bool on);
+void kernel_timer_reset();
+int kernel_timer_begin(const char *name);           // returns a slot or -1
+void kernel_timer_end(int slot, double algo_bytes);
+size_t kernel_timer_report(char *buf, size_t cap);  // "name launches ms bytes" lines
+
+struct KernelTimed {
+    int slot;
+    double bytes;
+    KernelTimed(const char *name, double algo_bytes) : slot(kernel_timer_begin(name)), bytes(algo_bytes) {}
+    ~KernelTimed() { kernel_timer_end(slot, bytes); }
+};
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
 // ---------------------------------------------------------------------------

@@ -120,6 +120,7 @@ void decimal_rows(const uint32_t *A, char *B, uint32_t N, uint32_t L, uint64_t s
                   uint64_t sB) {
     if (N == 0u || L == 0u || L_dec == 0u) return;
     cudaStream_t st = current_stream();
+    KernelTimed kt("decimal_leaf", 4.0 * N * L + (double)N * L_dec);
     const unsigned gt = grid_for(N, 128, kNumSMs * 32);
     const unsigned gw = grid_for(N, 4, kNumSMs * 32);
     if (L <= 8u) k_decimal_thread<8, NATURAL><<<gt, 128, 0, st>>>(A, B, N, L, sA, L_dec, sB);
@@ -172,6 +173,7 @@ static void extract_shifted(const BatchMPArray &src, uint32_t *dst, uint32_t d_s
                             uint32_t d_len, uint32_t rows, uint32_t shift, uint32_t off) {
     if (d_len == 0u || rows == 0u) return;
     const uint64_t total = (uint64_t)rows * d_len;
+    KernelTimed kt("decimal_extract", 8.0 * (double)total);
     k_extract_shifted<<<grid_for(total, 256, kNumSMs * 32), 256, 0, current_stream()>>>(
         src.data, src.stride, src.length, dst, d_stride, d_len, rows, shift, off);
     count_launch();
@@ -183,6 +185,7 @@ static void extract_low(const BatchMPArray &src, uint32_t *dst, uint32_t d_strid
     uint32_t mask = 0xffffffffu;
     if (valid_bits & 31u) mask = (1u << (valid_bits & 31u)) - 1u;
     const uint64_t total = (uint64_t)rows * d_len;
+    KernelTimed kt("decimal_extract", 8.0 * (double)total);
     k_extract_low<<<grid_for(total, 256, kNumSMs * 32), 256, 0, current_stream()>>>(
         src.data, src.stride, dst, d_stride, d_len, rows, mask);
     count_launch();
@@ -262,6 +265,7 @@ cudaError_t convert_decimal_precompute_powers(BatchMPContext *ctx, ConvertDecima
     if (powers[0].data == nullptr) return fail(0, cudaErrorMemoryAllocation);
     cudaError_t err = cudaMemcpyAsync(powers[0].data, base.data(), base.size() * 4,
                                       cudaMemcpyHostToDevice, current_stream());
+    note_h2d(base.size() * 4);
     if (err == cudaSuccess) err = cudaStreamSynchronize(current_stream());
     if (err != cudaSuccess) return fail(1, err);
     for (uint32_t l = 1; l < levels; ++l) {

@@ -151,6 +151,7 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
         cudaMemset2DAsync(C, sC * 4, 0, (size_t)(La + Lb) * 4, N, st);
         return;
     }
+    KernelTimed kt("schoolbook", 4.0 * N * (2.0 * (La + Lb)));
     // keep the longer operand as A for the register kernels
     if (La < Lb) {
         std::swap(A, B);

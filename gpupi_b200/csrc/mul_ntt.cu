@@ -18,6 +18,8 @@
 //   k_crt               Garner CRT to 96-bit coefficients, carry to limbs
 //                       (+ carry_fixup_kernel when a row spans several tiles)
 // Small products (K <= 4096) are one k_rows<from limbs> launch + k_crt.
+// Products longer than 2^27 limbs (up to 2^28) use two cosets of 2^27
+// points (see coef_residue), the third prime's 2-adicity being 27.
 //
 // The shared-memory butterflies are radix-2 levels separated by
 // __syncthreads; every DIF level needs one Montgomery product per pair.
@@ -38,6 +40,10 @@ struct NttParams {
     PrimeConsts pr[kPrimes];
     CrtConsts crt;
     Tables tab;
+    // two-coset split of a 2^28-point product: c1 = beta^(2^27) and
+    // (c1 - 1)^-1, both Montgomery form, per prime
+    uint32_t coset_c[kPrimes];
+    uint32_t coset_cm1_inv[kPrimes];
 };
 
 // ---------------------------------------------------------------------------
@@ -79,6 +85,11 @@ static NttParams make_params(const NTTPrecomputedTables &t) {
     P.tab.beta_lo = lv2 + 2 * kPrimes * kHiSize;
     P.tab.beta_hi = P.tab.beta_lo + 2 * kPrimes * kLoSize;
     P.tab.inv2n = reinterpret_cast<const uint32_t *>(t.inv2n_table);
+    for (int q = 0; q < kPrimes; ++q) {
+        const uint32_t c1 = h_pow(kGen[q], 1ull << kMaxLog, kP[q]);
+        P.coset_c[q] = h_mont(c1, kP[q]);
+        P.coset_cm1_inv[q] = h_mont(h_inv((c1 + kP[q] - 1u) % kP[q], kP[q]), kP[q]);
+    }
     return P;
 }
 
@@ -93,6 +104,7 @@ struct ColsArgs {
     uint32_t Lx;
     uint32_t *F;         // workspace of this operand: F[vrow][q][K]
     int log_k, log_s, log_r, log_tc;
+    int coset_bits;      // 1: vrow = 2*row + coset (2^28-point products)
 };
 
 template <bool FROM_LIMBS, bool INVERSE>
@@ -127,7 +139,21 @@ __global__ void __launch_bounds__(kThreads) k_cols(NttParams P, ColsArgs a) {
         const uint64_t i = ((uint64_t)r << log_cols) + c0 + c;
         uint32_t v;
         if (FROM_LIMBS) {
-            v = (i < a.Lx) ? reduce_limb(a.X[vrow * a.sX + i], p) : 0u;
+            const uint64_t row = vrow >> a.coset_bits;
+            const uint32_t *xr = a.X + row * a.sX;
+            v = (i < a.Lx) ? reduce_limb(xr[i], p) : 0u;
+            if (a.coset_bits) {
+                // a mod (x^K - c_j) = a_low + c_j * a_high, then scale by beta_j^i
+                const uint64_t i2 = i + K;
+                const uint32_t hi = (i2 < a.Lx) ? reduce_limb(xr[i2], p) : 0u;
+                if ((vrow & 1u) == 0u) {
+                    v = add_mod(v, hi, p);
+                } else {
+                    v = add_mod(v, mont_mul(hi, P.coset_c[q], p, pinv), p);
+                    v = mont_mul(v, root_pow(beta_lo_ptr(P.tab, 0, q), beta_hi_ptr(P.tab, 0, q), (uint32_t)i, p, pinv),
+                                 p, pinv);
+                }
+            }
         } else {
             v = F[i];
         }
@@ -164,6 +190,7 @@ struct RowsArgs {
     int log_k, log_c;
     int b_bcast;         // B row 0 serves every row
     int square;          // B is A
+    int coset_bits;      // virtual rows are (row, coset) pairs
 };
 
 template <bool FROM_LIMBS>
@@ -180,7 +207,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(NttParams P, RowsArgs a) {
     const uint32_t nseg = 1u << (a.log_k - a.log_c);
     const uint32_t seg = (uint32_t)(b % nseg);
     const uint64_t vrow = b / nseg;
-    const uint64_t brow = a.b_bcast ? 0 : vrow;
+    const uint64_t brow = a.b_bcast ? (vrow & ((1u << a.coset_bits) - 1u)) : vrow;
     const uint32_t p = P.pr[q].p, pinv = P.pr[q].pinv;
     const uint64_t K = 1ull << a.log_k;
     const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + q);
@@ -241,14 +268,35 @@ struct CrtArgs {
     uint32_t *flags;
 };
 
+// Residue mod p_q of convolution coefficient n.  Without cosets it is read
+// directly.  With two cosets (K = transform length, product length <= 2K) the
+// row holds r0 = C mod (x^K - 1) and beta^i * r1, r1 = C mod (x^K - c1):
+// C_high = (r1 - r0) / (c1 - 1), C_low = r0 - C_high.
+template <bool COSET>
+__device__ __forceinline__ uint32_t coef_residue(const NttParams &P, const uint32_t *F0, uint64_t K, int q,
+                                                 uint64_t n) {
+    if (!COSET) return F0[(uint64_t)q * K + n];
+    const uint32_t p = P.pr[q].p, pinv = P.pr[q].pinv;
+    const uint64_t i = n & (K - 1);
+    const uint32_t r0 = F0[(uint64_t)q * K + i];
+    const uint32_t s1 = F0[3 * K + (uint64_t)q * K + i];
+    const uint32_t r1 =
+        mont_mul(s1, root_pow(beta_lo_ptr(P.tab, 1, q), beta_hi_ptr(P.tab, 1, q), (uint32_t)i, p, pinv), p, pinv);
+    const uint32_t hi = mont_mul(sub_mod(r1, r0, p), P.coset_cm1_inv[q], p, pinv);
+    return (n >= K) ? hi : sub_mod(r0, hi, p);
+}
+
+template <bool COSET>
 __device__ __forceinline__ void crt_chunk(const NttParams &P, const uint32_t *F0, uint64_t K,
                                           uint32_t Lc, int64_t base, uint32_t (&S)[kCrtV + 3]) {
     uint32_t c[kCrtV][3];
+    const uint64_t span = COSET ? 2 * K : K;
 #pragma unroll
     for (int v = 0; v < kCrtV; ++v) {
         const int64_t i = base + v;
-        if (i >= 0 && (uint64_t)i < K && i < (int64_t)Lc) {
-            garner(P, F0[i], F0[K + i], F0[2 * K + i], c[v]);
+        if (i >= 0 && (uint64_t)i < span && i < (int64_t)Lc) {
+            garner(P, coef_residue<COSET>(P, F0, K, 0, i), coef_residue<COSET>(P, F0, K, 1, i),
+                   coef_residue<COSET>(P, F0, K, 2, i), c[v]);
         } else {
             c[v][0] = c[v][1] = c[v][2] = 0u;
         }
@@ -256,23 +304,24 @@ __device__ __forceinline__ void crt_chunk(const NttParams &P, const uint32_t *F0
     chunk_sum3<kCrtV>(c, S);
 }
 
+template <bool COSET>
 __global__ void __launch_bounds__(kThreads) k_crt(NttParams P, CrtArgs a) {
     __shared__ uint32_t sg[kThreads / 32], sp[kThreads / 32], spre[kThreads / 32];
     const uint32_t tile = blockIdx.x;
     const uint64_t row = tile / a.tiles;
     const uint32_t t = tile - (uint32_t)row * a.tiles;
     const uint64_t K = 1ull << a.log_k;
-    const uint32_t *F0 = a.F + row * 3 * K;
+    const uint32_t *F0 = a.F + row * (COSET ? 6 : 3) * K;
     const int64_t base = (int64_t)t * kCrtSpan + threadIdx.x * kCrtV;
     uint32_t S[kCrtV + 3];
-    crt_chunk(P, F0, K, a.Lc, base, S);
+    crt_chunk<COSET>(P, F0, K, a.Lc, base, S);
     uint32_t H[3];
     H[0] = __shfl_up_sync(0xffffffffu, S[kCrtV], 1);
     H[1] = __shfl_up_sync(0xffffffffu, S[kCrtV + 1], 1);
     H[2] = __shfl_up_sync(0xffffffffu, S[kCrtV + 2], 1);
     if (lane_id() == 0) {
         uint32_t Sp[kCrtV + 3];
-        crt_chunk(P, F0, K, a.Lc, base - kCrtV, Sp);
+        crt_chunk<COSET>(P, F0, K, a.Lc, base - kCrtV, Sp);
         H[0] = Sp[kCrtV];
         H[1] = Sp[kCrtV + 1];
         H[2] = Sp[kCrtV + 2];
@@ -324,6 +373,12 @@ static void launch_cols(bool from_limbs, bool inverse, const NttParams &P, const
     const uint64_t nseg = 1ull << (a.log_k - a.log_s);
     const uint64_t blocks = vrows * kPrimes * nseg * ctiles;
     const size_t smem = ((size_t(1) << (a.log_r + a.log_tc)) + (size_t(1) << (a.log_r - 1))) * 4;
+    // algorithmic bytes: 12 B per coefficient (3 primes x 4 B) read and written;
+    // the first pass reads each limb once instead
+    const double K = (double)(1ull << a.log_k);
+    const double bytes = from_limbs ? (4.0 * a.Lx * (double)(vrows >> a.coset_bits) + 12.0 * K * (double)vrows)
+                                    : 24.0 * K * (double)vrows;
+    KernelTimed kt(from_limbs ? "ntt_cols_fwd_first" : (inverse ? "ntt_cols_inv" : "ntt_cols_fwd"), bytes);
     if (from_limbs) {
         set_smem(k_cols<true, false>, smem);
         k_cols<true, false><<<(unsigned)blocks, kThreads, smem, st>>>(P, a);
@@ -362,23 +417,28 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         cudaMemset2DAsync(C, sC * 4, 0, (size_t)Lc * 4, N, st);
         return;
     }
-    const int log_k = transform_log(La, Lb);
-    if (log_k > kMaxLog) {
-        fprintf(stderr, "gpupi_b200: product of %u limbs exceeds the 2^27-point transform\n", Lc);
+    const int log_total = transform_log(La, Lb);
+    if (log_total > kMaxLog + 1) {
+        fprintf(stderr, "gpupi_b200: product of %u limbs exceeds the 2^28-point limit\n", Lc);
         return;
     }
+    // Above 2^27 points the product is split into two cosets of 2^27 points.
+    const int cb = (log_total > kMaxLog) ? 1 : 0;
+    const int log_k = log_total - cb;
     const uint64_t K = 1ull << log_k;
+    const uint64_t VR = (uint64_t)N << cb;   // virtual rows (row, coset)
     const bool square = (A == B && La == Lb && sA == sB);
     const bool bcast = (!square && sB == 0u && N > 1u);
     uint32_t *FA = ws;
-    uint32_t *FB = square ? FA : ws + (uint64_t)N * 3 * K;
+    uint32_t *FB = square ? FA : ws + VR * 3 * K;
     const uint64_t tiles = ((uint64_t)Lc + kCrtSpan - 1) / kCrtSpan;
-    uint32_t *flags = ws + 2ull * N * 3 * K;
+    uint32_t *flags = ws + 2ull * VR * 3 * K;
 
     if (log_k <= 12) {
-        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_k, bcast ? 1 : 0, square ? 1 : 0};
+        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_k, bcast ? 1 : 0, square ? 1 : 0, 0};
         const size_t smem = (size_t)3 * K * 4;
         set_smem(k_rows<true>, smem);
+        KernelTimed kt("ntt_local", 4.0 * N * ((double)La + (square ? 0 : Lb)) + 12.0 * K * N);
         k_rows<true><<<(unsigned)(N * kPrimes), kThreads, smem, st>>>(P, r);
         count_launch();
     } else {
@@ -400,32 +460,37 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
             const uint64_t sX = op == 0 ? sA : sB;
             const uint32_t Lx = op == 0 ? La : Lb;
             uint32_t *F = op == 0 ? FA : FB;
-            const uint64_t vrows = (op == 1 && bcast) ? 1 : N;
+            const uint64_t vrows = (op == 1 && bcast) ? (1ull << cb) : VR;
             int log_s = log_k;
             for (int ps = 0; ps < npass; ++ps) {
-                ColsArgs a{X, sX, Lx, F, log_k, log_s, passes[ps], 0};
+                ColsArgs a{X, sX, Lx, F, log_k, log_s, passes[ps], 0, cb};
                 a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
                 launch_cols(ps == 0, false, P, a, vrows, st);
                 log_s -= passes[ps];
             }
         }
-        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_c, bcast ? 1 : 0, square ? 1 : 0};
+        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_c, bcast ? 1 : 0, square ? 1 : 0, cb};
         const size_t smem = (size_t)3 * (1u << log_c) * 4;
         set_smem(k_rows<false>, smem);
-        const uint64_t blocks = (uint64_t)N * kPrimes * (K >> log_c);
+        const uint64_t blocks = VR * kPrimes * (K >> log_c);
+        KernelTimed kt("ntt_rows_fused", 12.0 * (double)K * ((square ? 2.0 : 3.0) * (double)VR));
         k_rows<false><<<(unsigned)blocks, kThreads, smem, st>>>(P, r);
         count_launch();
         // inverse column passes, innermost first
         int log_s = log_c;
         for (int ps = npass - 1; ps >= 0; --ps) {
             log_s += passes[ps];
-            ColsArgs a{nullptr, 0, 0, FA, log_k, log_s, passes[ps], 0};
+            ColsArgs a{nullptr, 0, 0, FA, log_k, log_s, passes[ps], 0, 0};
             a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
-            launch_cols(false, true, P, a, N, st);
+            launch_cols(false, true, P, a, VR, st);
         }
     }
     CrtArgs c{FA, log_k, C, sC, Lc, (uint32_t)tiles, flags};
-    k_crt<<<(unsigned)(N * tiles), kThreads, 0, st>>>(P, c);
+    KernelTimed kt("ntt_crt_carry", 12.0 * (double)Lc * N + 4.0 * (double)Lc * N);
+    if (cb)
+        k_crt<true><<<(unsigned)(N * tiles), kThreads, 0, st>>>(P, c);
+    else
+        k_crt<false><<<(unsigned)(N * tiles), kThreads, 0, st>>>(P, c);
     count_launch();
     if (tiles > 1) launch_carry_fixup(false, C, sC, N, Lc, (uint32_t)tiles, kCrtSpan, flags, st);
 }

@@ -350,6 +350,7 @@ static cudaError_t sqrt_10005(BatchMPContext *ctx, Profiler *pr, int target, Buf
     const uint32_t p15 = 4001u, q15 = 40u;
     TRY(cudaMemcpyAsync(pbuf.p, &p15, 4, cudaMemcpyHostToDevice, st));
     TRY(cudaMemcpyAsync(qbuf.p, &q15, 4, cudaMemcpyHostToDevice, st));
+    note_h2d(8);
     TRY(cudaStreamSynchronize(st));
     P = BatchMPArray{pbuf.p, 1, 1, 1};
     Q = BatchMPArray{qbuf.p, 1, 1, 1};
@@ -427,6 +428,7 @@ static void divmod_pow2(uint32_t e, std::vector<uint32_t> v, std::vector<uint32_
             rem = cur % v[0];
         }
         r.assign(1, (uint32_t)rem);
+        while (q.size() > 1 && q.back() == 0u) q.pop_back();
         return;
     }
     const int s = __builtin_clz(v[n - 1]);
@@ -531,6 +533,7 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
         std::vector<uint32_t> hx(x0.length);
         if (x0.length)
             TRY(cudaMemcpyAsync(hx.data(), x0.data, (size_t)x0.length * 4, cudaMemcpyDeviceToHost, st));
+        note_d2h((size_t)x0.length * 4);
         TRY(cudaStreamSynchronize(st));
         std::vector<uint32_t> hq, hr;
         divmod_pow2((uint32_t)L0, hx, hq, hr);
@@ -540,6 +543,7 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
         hr.resize(res.stride, 0u);
         TRY(cudaMemcpyAsync(y0.data, hq.data(), (size_t)y0.stride * 4, cudaMemcpyHostToDevice, st));
         TRY(cudaMemcpyAsync(res.data, hr.data(), (size_t)res.stride * 4, cudaMemcpyHostToDevice, st));
+        note_h2d((size_t)(y0.stride + res.stride) * 4);
         TRY(cudaStreamSynchronize(st));
     }
     TRY(res.compact(ctx));
@@ -557,6 +561,7 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
         TRY(p_sub(ctx, pr, res1m, x2y1, res1m, "res1_m", dg));
         uint32_t top = 0u;
         TRY(cudaMemcpyAsync(&top, res1m.data + res1m.length - 1, 4, cudaMemcpyDeviceToHost, st));
+        note_d2h(4);
         TRY(cudaStreamSynchronize(st));
         const bool neg = top >= 0x80000000u;
         if (neg) {
@@ -638,6 +643,7 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     if (Qtf.length > 0u) {
         uint32_t topl = 0u;
         TRY(cudaMemcpyAsync(&topl, Qtf.data + Qtf.length - 1, 4, cudaMemcpyDeviceToHost, st));
+        note_d2h(4);
         TRY(cudaStreamSynchronize(st));
         qbits = (Qtf.length - 1u) * 32u + (topl ? 32u - (uint32_t)__builtin_clz(topl) : 0u);
     }
@@ -696,6 +702,9 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     const uint32_t requested = req.digits;
     uint32_t leaf = 0u;
     const uint32_t convert = round_up_decimal_digits(requested, &leaf);
+    // round_up_decimal_digits leaves the reference's global leaf size (477)
+    // untouched when nothing is requested (pi_bs_gpu.cu:155, 924-928)
+    if (leaf == 0u) leaf = 477u;
     const uint32_t prec = prec_limbs_for_digits(requested);
     out.target_digits = requested;
     out.convert_digits = convert;
@@ -708,6 +717,15 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
         if (!ctx) return cudaErrorMemoryAllocation;
     }
     cudaStream_t st = current_stream();
+    {
+        // keep freed blocks in the stream-ordered pool across synchronisations
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     Profiler prof;
     prof.on = req.profile_stages;
     const uint32_t levels = convert ? (uint32_t)__builtin_ctz(convert / leaf) : 0u;
@@ -740,14 +758,21 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     if (err == cudaSuccess) err = cudaEventElapsedTime(&out.elapsed_ms, e0, e1);
     out.ret_len = RET.length;
     out.workspace_bytes = batch_mp_workspace_size(ctx);
-    if (err == cudaSuccess) {
+    if (err == cudaSuccess && !req.device_only) {
         out.ret.resize(RET.length);
-        if (RET.length)
+        if (RET.length) {
             err = cudaMemcpyAsync(out.ret.data(), RET.data, (size_t)RET.length * 4, cudaMemcpyDeviceToHost, st);
+            note_d2h((size_t)RET.length * 4);
+        }
         const uint32_t want = std::min(requested, req.copy_digits);
         if (err == cudaSuccess && want > 0u) {
-            out.digits.resize(want);
-            err = cudaMemcpyAsync(&out.digits[0], d_digits, want, cudaMemcpyDeviceToHost, st);
+            char *dst = req.host_digits;
+            if (!dst) {
+                out.digits.resize(want);
+                dst = &out.digits[0];
+            }
+            err = cudaMemcpyAsync(dst, d_digits, want, cudaMemcpyDeviceToHost, st);
+            note_d2h(want);
         }
         if (err == cudaSuccess && req.copy_digits < requested && requested > 0u) {
             // tail for the --benchmark preview

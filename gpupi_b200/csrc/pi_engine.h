@@ -23,6 +23,8 @@ struct PiRequest {
     bool profile_stages = false;    // time every op (serialises the run)
     uint32_t copy_digits = 0;       // how many leading digits to copy to the host
     BatchMPContext *ctx = nullptr;  // reuse a context (keeps its workspace); null = private
+    bool device_only = false;       // leave RET and the digits on the device (no host copies)
+    char *host_digits = nullptr;    // caller buffer (>= copy_digits bytes, may be pinned) for the digits
 };
 
 struct PiOutput {
@@ -32,7 +34,7 @@ struct PiOutput {
     float elapsed_ms = 0.f;
     size_t workspace_bytes = 0;
     std::vector<uint32_t> ret;      // RET limbs (little endian)
-    std::string digits;             // first copy_digits digits
+    std::string digits;             // first copy_digits digits (unless PiRequest::host_digits)
     std::string tail;               // last 64 requested digits when not all were copied
     std::vector<StageEntry> stages;
 };

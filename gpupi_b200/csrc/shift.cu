@@ -62,6 +62,7 @@ void batch_shift_bits(const uint32_t *A, uint32_t *B, uint32_t N, uint32_t L_in,
     if (N == 0u || L_out == 0u) return;
     const uint32_t chunks = (L_out + kShiftPerThread - 1) / kShiftPerThread;
     const uint64_t total = (uint64_t)N * chunks;
+    KernelTimed kt("shift", 8.0 * N * (double)L_out);
     shift_bits_kernel<<<grid_for(total, 256, kNumSMs * 32), 256, 0, current_stream()>>>(
         A, B, N, L_in, L_out, stride_in, stride_out, shift_bits, chunks);
     GPUPI_LAUNCH_CHECK();

@@ -91,12 +91,24 @@ int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *d_X, uint32_t L_x, uin
 
 /* Whole pi_bs_gpu pipeline (pi_bs_gpu.cu:2073-2431, main_fractional).
  * h_ret (capacity ret_cap limbs) receives RET, h_digits (capacity digits_cap)
- * the first min(digits, digits_cap) decimal digits after "3.".  Either may be
- * null.  info[0..7] receives: convert_digits, RET length, elapsed ms on the
- * device (float bits), workspace MB, number of profiled stages, leaf digits,
- * 0, 0.  flags bit 0 = profile every stage. */
+ * the first min(digits, digits_cap) decimal digits after "3." (copied
+ * straight from the device; pinned memory makes that copy fastest).  Either
+ * may be null.  info[0..7] receives: convert_digits, RET length, elapsed ms
+ * on the device (float bits), workspace MB, number of profiled stages, leaf
+ * digits, 0, 0.  flags bit 0 = profile every stage, bit 1 = keep RET and the
+ * digits on the device (no host copies). */
 int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
                      char *h_digits, size_t digits_cap, uint32_t *info);
+
+/* Per-kernel timing: CUDA events around each launch on the current stream,
+ * with the launch's algorithmic HBM bytes.  The report has one line per
+ * kernel family: "name launches total_ms total_bytes". */
+int gpupi_timer_enable(int on);
+int gpupi_timer_reset(void);
+size_t gpupi_timer_report(char *buf, size_t cap);
+
+/* Cumulative host->device and device->host bytes copied by the library. */
+int gpupi_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 
 /* Multiply crossover: largest L_a + L_b computed by schoolbook (<= 1024). */
 int gpupi_set_mul_crossover(uint32_t max_school_len);

@@ -11,7 +11,11 @@ Python integers.  File:line citations are into the gpupi project.
 """
 from __future__ import annotations
 
+import sys
+
 import numpy as np
+
+sys.set_int_max_str_digits(0)   # decimal strings of very long integers
 
 M32 = (1 << 32) - 1
 

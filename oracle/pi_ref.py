@@ -14,7 +14,10 @@ References are ``file:line`` inside the gpupi project.
 """
 from __future__ import annotations
 
+import sys
 from dataclasses import dataclass
+
+sys.set_int_max_str_digits(0)   # decimal strings of very long integers
 
 MASK32 = (1 << 32) - 1
 VALIDATION_MOD = 1_000_000_007          # pi_bs_gpu.cu:149

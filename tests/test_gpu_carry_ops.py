@@ -57,9 +57,9 @@ def test_long_carry_chain(ctx, L):
     ctx.add(N, dA.ptr, L, L, dB.ptr, L, L, dC.ptr, L + 1, L + 1)
     assert np.array_equal(dC.numpy(), ref.add(N, A, L, L, B, L, L, C, L + 1, L + 1))
     Z = np.zeros(N * L, dtype=np.uint32)
-    dZ = to_dev(Z)
-    ctx.sub(N, dZ.ptr, L, L, dB.ptr, L, L, dC.ptr, L, L + 1)
-    assert np.array_equal(dC.numpy(), ref.sub(N, Z, L, L, B, L, L, C, L, L + 1))
+    dZ, dD = to_dev(Z), to_dev(C)
+    ctx.sub(N, dZ.ptr, L, L, dB.ptr, L, L, dD.ptr, L, L + 1)
+    assert np.array_equal(dD.numpy(), ref.sub(N, Z, L, L, B, L, L, C, L, L + 1))
 
 
 def test_carry_chain_mixed_runs(ctx):

@@ -103,3 +103,12 @@ def test_uneven_pairs_sample(ctx):
         La = int(2 ** rng.uniform(3, 12))
         Lb = int(2 ** rng.uniform(3, 12))
         _check_mul(ctx, 1, La, Lb, La, Lb, La + Lb, rng)
+
+
+def test_ntt_two_cosets(ctx):
+    """Products longer than 2^27 limbs: the residues mod x^K - 1 and
+    x^K - beta^K (K = 2^27) are recombined per coefficient."""
+    rng = np.random.default_rng(28)
+    L = (1 << 26) + 1
+    _check_mul(ctx, 1, L, L, L, L, 2 * L, rng, path="ntt")
+    _check_mul(ctx, 1, L + 1000, L - 999, L + 1000, L - 999, 2 * L + 1, rng, path="ntt", extreme=True)
