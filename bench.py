@@ -258,6 +258,43 @@ def run_ours(args, ws, rank, local):
     ctx.close()
 
 
+def run_ntt(args, ws, rank, local):
+    """One batched NTT product of two ntt_limbs-limb operands per step (the
+    2^27 x 2^27-limb configuration by default), operands resident in HBM."""
+    import torch
+    import gpupi_b200 as g
+
+    torch.cuda.set_device(local)
+    ctx = g.Context()
+    L = args.ntt_limbs
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0x4D595DF4)
+    A = torch.randint(-2 ** 31, 2 ** 31 - 1, (L,), dtype=torch.int32, device="cuda", generator=gen)
+    B = torch.randint(-2 ** 31, 2 ** 31 - 1, (L,), dtype=torch.int32, device="cuda", generator=gen)
+    C = torch.zeros(2 * L, dtype=torch.int32, device="cuda")
+    for _ in range(args.warmup):
+        ctx.mul(1, A.data_ptr(), L, L, B.data_ptr(), L, L, C.data_ptr(), 2 * L, 2 * L)
+    torch.cuda.synchronize()
+    g.timer_reset()
+    g.timer_enable(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        ctx.mul(1, A.data_ptr(), L, L, B.data_ptr(), L, L, C.data_ptr(), 2 * L, 2 * L)
+    e1.record()
+    torch.cuda.synchronize()
+    g.timer_enable(False)
+    ms = _max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
+    fam = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
+               "GBps": v[2] / (v[1] * 1e-3) / 1e9 if v[1] > 0 else None} for k, v in g.timer_report().items()}
+    if rank == 0:
+        print(json.dumps({"metric": f"ms per {L}x{L}-limb NTT product", "value": ms, "unit": "ms",
+                          "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
+                          "a_b_ret_GBps": 16.0 * L / (ms * 1e-3) / 1e9, "kernel_families": fam}), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -266,6 +303,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--digits", type=int, default=1_000_000_000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--workload", choices=["pi", "ntt"], default="pi",
+                    help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step")
+    ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
     args = ap.parse_args()
     ws, rank, local = _dist()
     if ws > 1:
@@ -277,6 +317,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, ws, rank)
+        elif args.workload == "ntt":
+            run_ntt(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

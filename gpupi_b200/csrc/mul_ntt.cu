@@ -28,6 +28,7 @@
 #include "batch_mul_ntt.h"
 
 #include <stdio.h>
+#include <stdlib.h>
 #include <vector>
 
 namespace gpupi {
@@ -88,7 +89,8 @@ static NttParams make_params(const NTTPrecomputedTables &t) {
     for (int q = 0; q < kPrimes; ++q) {
         const uint32_t c1 = h_pow(kGen[q], 1ull << kMaxLog, kP[q]);
         P.coset_c[q] = h_mont(c1, kP[q]);
-        P.coset_cm1_inv[q] = h_mont(h_inv((c1 + kP[q] - 1u) % kP[q], kP[q]), kP[q]);
+        const uint32_t cm1 = (c1 == 0u) ? kP[q] - 1u : c1 - 1u;   // c1 - 1 mod p without 32-bit overflow
+        P.coset_cm1_inv[q] = h_mont(h_inv(cm1, kP[q]), kP[q]);
     }
     return P;
 }
@@ -97,6 +99,15 @@ static NttParams make_params(const NTTPrecomputedTables &t) {
 // Kernels
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
+
+// Per-prime constants chosen by value (indexing the kernel-parameter arrays
+// with a run-time prime index would force a local-memory copy).
+__device__ __forceinline__ PrimeConsts prime_of(const NttParams &P, int q) {
+    return q == 0 ? P.pr[0] : (q == 1 ? P.pr[1] : P.pr[2]);
+}
+__device__ __forceinline__ uint32_t sel3(const uint32_t (&v)[kPrimes], int q) {
+    return q == 0 ? v[0] : (q == 1 ? v[1] : v[2]);
+}
 
 struct ColsArgs {
     const uint32_t *X;   // limbs (first forward pass only)
@@ -124,7 +135,8 @@ __global__ void __launch_bounds__(kThreads) k_cols(NttParams P, ColsArgs a) {
     b /= ctiles;
     const uint32_t seg = (uint32_t)(b % nseg);
     const uint64_t vrow = b / nseg;
-    const uint32_t p = P.pr[q].p, pinv = P.pr[q].pinv;
+    const PrimeConsts pc = prime_of(P, q);
+    const uint32_t p = pc.p, pinv = pc.pinv;
     const int dir = INVERSE ? 1 : 0;
     const uint64_t K = 1ull << a.log_k;
     const uint32_t *twhi = tw_hi_ptr(P.tab, dir, q);
@@ -149,7 +161,7 @@ __global__ void __launch_bounds__(kThreads) k_cols(NttParams P, ColsArgs a) {
                 if ((vrow & 1u) == 0u) {
                     v = add_mod(v, hi, p);
                 } else {
-                    v = add_mod(v, mont_mul(hi, P.coset_c[q], p, pinv), p);
+                    v = add_mod(v, mont_mul(hi, sel3(P.coset_c, q), p, pinv), p);
                     v = mont_mul(v, root_pow(beta_lo_ptr(P.tab, 0, q), beta_hi_ptr(P.tab, 0, q), (uint32_t)i, p, pinv),
                                  p, pinv);
                 }
@@ -208,7 +220,8 @@ __global__ void __launch_bounds__(kThreads) k_rows(NttParams P, RowsArgs a) {
     const uint32_t seg = (uint32_t)(b % nseg);
     const uint64_t vrow = b / nseg;
     const uint64_t brow = a.b_bcast ? (vrow & ((1u << a.coset_bits) - 1u)) : vrow;
-    const uint32_t p = P.pr[q].p, pinv = P.pr[q].pinv;
+    const PrimeConsts pc = prime_of(P, q);
+    const uint32_t p = pc.p, pinv = pc.pinv;
     const uint64_t K = 1ull << a.log_k;
     const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + q);
     const uint32_t *thf = tw_hi_ptr(P.tab, 0, q);
@@ -239,6 +252,164 @@ __global__ void __launch_bounds__(kThreads) k_rows(NttParams P, RowsArgs a) {
     __syncthreads();
     tile_transform<true>(SA, a.log_c, 0, twi, p, pinv);
     for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) a.FA[offA + i] = SA[i];
+}
+
+// ---------------------------------------------------------------------------
+// Register-stage kernels (ntt_core.cuh: Stage / run_stages).  Same arithmetic
+// as k_cols / k_rows, with 16 residues per thread and shared memory touched
+// only between stages of up to four radix-2 levels.
+// ---------------------------------------------------------------------------
+constexpr int kTile = 4096;                    // elements per register-stage CTA tile
+constexpr int kTilePad = kTile + kTile / 32;   // padded shared-memory words
+
+__device__ __forceinline__ uint32_t load_operand(const NttParams &P, const ColsArgs &a, const uint32_t *F,
+                                                 uint64_t vrow, uint64_t i, uint64_t K, int q, uint32_t p,
+                                                 uint32_t pinv) {
+    (void)F;
+    const uint64_t row = vrow >> a.coset_bits;
+    const uint32_t *xr = a.X + row * a.sX;
+    uint32_t v = (i < a.Lx) ? reduce_limb(xr[i], p) : 0u;
+    if (a.coset_bits) {
+        // a mod (x^K - c_j) = a_low + c_j * a_high, then scale by beta_j^i
+        const uint64_t i2 = i + K;
+        const uint32_t hi = (i2 < a.Lx) ? reduce_limb(xr[i2], p) : 0u;
+        if ((vrow & 1u) == 0u) {
+            v = add_mod(v, hi, p);
+        } else {
+            v = add_mod(v, mont_mul(hi, sel3(P.coset_c, q), p, pinv), p);
+            v = mont_mul(v, root_pow(beta_lo_ptr(P.tab, 0, q), beta_hi_ptr(P.tab, 0, q), (uint32_t)i, p, pinv), p,
+                         pinv);
+        }
+    }
+    return v;
+}
+
+// Column pass: R = 2^LOG_R (<= 512) points per column, TC = 4096 / R columns.
+template <int LOG_R, bool FROM_LIMBS, bool INVERSE>
+__global__ void __launch_bounds__(kThreads) k_cols_r(NttParams P, ColsArgs a) {
+    constexpr int LOG_TC = 12 - LOG_R;
+    constexpr int NS = StagePlan<LOG_R>::n;
+    using First = typename ExecStage<LOG_R, LOG_TC, INVERSE, 0>::S;
+    using Last = typename ExecStage<LOG_R, LOG_TC, INVERSE, NS - 1>::S;
+    __shared__ uint32_t Sm[kTilePad];
+    __shared__ uint32_t tw[(1 << LOG_R) / 2 > 0 ? (1 << LOG_R) / 2 : 1];
+    const int log_cols = a.log_s - LOG_R;
+    const uint32_t ctiles = 1u << (log_cols - LOG_TC);
+    const uint32_t nseg = 1u << (a.log_k - a.log_s);
+    uint64_t b = blockIdx.x;
+    const int q = (int)(b % kPrimes);
+    b /= kPrimes;
+    const uint32_t ct = (uint32_t)(b % ctiles);
+    b /= ctiles;
+    const uint32_t seg = (uint32_t)(b % nseg);
+    const uint64_t vrow = b / nseg;
+    const PrimeConsts pc = prime_of(P, q);
+    const uint32_t p = pc.p, pinv = pc.pinv;
+    const int dir = INVERSE ? 1 : 0;
+    const uint64_t K = 1ull << a.log_k;
+    const uint32_t *twhi = tw_hi_ptr(P.tab, dir, q);
+    const uint32_t *twlo = tw_lo_ptr(P.tab, dir, q);
+    for (uint32_t e = threadIdx.x; e < (1u << LOG_R) / 2; e += kThreads) tw[e] = __ldg(twhi + (e << (13 - LOG_R)));
+    uint32_t *F = a.F + vrow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << a.log_s);
+    const uint32_t c0 = ct << LOG_TC;
+    const int twist_shift = kMaxLog - a.log_s;
+    const uint32_t t = threadIdx.x;
+    uint32_t x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t pos, c;
+        First::elem(t, j, pos, c);
+        const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+        uint32_t v = FROM_LIMBS ? load_operand(P, a, F, vrow, i, K, q, p, pinv) : F[i];
+        if (INVERSE) {
+            const uint32_t E = ((c0 + c) * bitrev(pos, LOG_R)) << twist_shift;
+            v = mont_mul(v, root_pow(twlo, twhi, E, p, pinv), p, pinv);
+        }
+        x[j] = v;
+    }
+    __syncthreads();   // twiddle table ready
+    run_stages<LOG_R, LOG_TC, INVERSE, 0>(x, Sm, t, tw, p, pinv);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t pos, c;
+        Last::elem(t, j, pos, c);
+        const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+        uint32_t v = x[j];
+        if (!INVERSE) {
+            const uint32_t E = ((c0 + c) * bitrev(pos, LOG_R)) << twist_shift;
+            v = mont_mul(v, root_pow(twlo, twhi, E, p, pinv), p, pinv);
+        }
+        F[i] = v;
+    }
+}
+
+// Fused row pass on C = 2^LOG_C points (T = C/16 threads): forward stages of
+// A then B (A stays in registers while B reuses the shared tile), pointwise
+// product * scale, inverse stages.  The last forward and the first inverse
+// stage share one thread mapping, so the product never leaves registers.
+template <int LOG_C, bool FROM_LIMBS>
+__global__ void __launch_bounds__(kThreads) k_rows_r(NttParams P, RowsArgs a) {
+    constexpr int C = 1 << LOG_C;
+    constexpr int NS = StagePlan<LOG_C>::n;
+    using First = typename ExecStage<LOG_C, 0, false, 0>::S;
+    using Mid = typename ExecStage<LOG_C, 0, false, NS - 1>::S;
+    using Out = typename ExecStage<LOG_C, 0, true, NS - 1>::S;
+    __shared__ uint32_t Sm[C + C / 32];
+    __shared__ uint32_t twf[C / 2], twi[C / 2];
+    uint64_t b = blockIdx.x;
+    const int q = (int)(b % kPrimes);
+    b /= kPrimes;
+    const uint32_t nseg = 1u << (a.log_k - LOG_C);
+    const uint32_t seg = (uint32_t)(b % nseg);
+    const uint64_t vrow = b / nseg;
+    const uint64_t brow = a.b_bcast ? (vrow & ((1u << a.coset_bits) - 1u)) : vrow;
+    const PrimeConsts pc = prime_of(P, q);
+    const uint32_t p = pc.p, pinv = pc.pinv;
+    const uint64_t K = 1ull << a.log_k;
+    const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + q);
+    const uint32_t *thf = tw_hi_ptr(P.tab, 0, q);
+    const uint32_t *thi = tw_hi_ptr(P.tab, 1, q);
+    for (uint32_t e = threadIdx.x; e < C / 2; e += blockDim.x) {
+        twf[e] = __ldg(thf + (e << (13 - LOG_C)));
+        twi[e] = __ldg(thi + (e << (13 - LOG_C)));
+    }
+    const uint64_t offA = vrow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << LOG_C);
+    const uint64_t offB = brow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << LOG_C);
+    const uint32_t t = threadIdx.x;
+    uint32_t xa[16], xb[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t pos, c;
+        First::elem(t, j, pos, c);
+        if (FROM_LIMBS) {
+            xa[j] = (pos < a.La) ? reduce_limb(a.A[vrow * a.sA + pos], p) : 0u;
+            xb[j] = (!a.square && pos < a.Lb) ? reduce_limb(a.B[brow * a.sB + pos], p) : 0u;
+        } else {
+            xa[j] = a.FA[offA + pos];
+            xb[j] = a.square ? 0u : a.FB[offB + pos];
+        }
+    }
+    __syncthreads();
+    run_stages<LOG_C, 0, false, 0>(xa, Sm, t, twf, p, pinv);
+    if (!a.square) {
+        // the tile is free again: every thread has passed the last stage's loads
+        __syncthreads();
+        run_stages<LOG_C, 0, false, 0>(xb, Sm, t, twf, p, pinv);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const uint32_t y = a.square ? xa[j] : xb[j];
+        xa[j] = mont_mul(mont_mul(xa[j], y, p, pinv), scale, p, pinv);
+    }
+    __syncthreads();
+    run_stages<LOG_C, 0, true, 0>(xa, Sm, t, twi, p, pinv);
+    (void)sizeof(Mid);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t pos, c;
+        Out::elem(t, j, pos, c);
+        a.FA[offA + pos] = xa[j];
+    }
 }
 
 __device__ __forceinline__ void garner(const NttParams &P, uint32_t r0, uint32_t r1, uint32_t r2,
@@ -276,13 +447,14 @@ template <bool COSET>
 __device__ __forceinline__ uint32_t coef_residue(const NttParams &P, const uint32_t *F0, uint64_t K, int q,
                                                  uint64_t n) {
     if (!COSET) return F0[(uint64_t)q * K + n];
-    const uint32_t p = P.pr[q].p, pinv = P.pr[q].pinv;
+    const PrimeConsts pc = prime_of(P, q);
+    const uint32_t p = pc.p, pinv = pc.pinv;
     const uint64_t i = n & (K - 1);
     const uint32_t r0 = F0[(uint64_t)q * K + i];
     const uint32_t s1 = F0[3 * K + (uint64_t)q * K + i];
     const uint32_t r1 =
         mont_mul(s1, root_pow(beta_lo_ptr(P.tab, 1, q), beta_hi_ptr(P.tab, 1, q), (uint32_t)i, p, pinv), p, pinv);
-    const uint32_t hi = mont_mul(sub_mod(r1, r0, p), P.coset_cm1_inv[q], p, pinv);
+    const uint32_t hi = mont_mul(sub_mod(r1, r0, p), sel3(P.coset_cm1_inv, q), p, pinv);
     return (n >= K) ? hi : sub_mod(r0, hi, p);
 }
 
@@ -392,6 +564,57 @@ static void launch_cols(bool from_limbs, bool inverse, const NttParams &P, const
     count_launch();
 }
 
+static bool use_radix2() {
+    static const bool v = [] {
+        const char *e = getenv("GPUPI_NTT_RADIX2");
+        return e && e[0] == '1';
+    }();
+    return v;
+}
+
+template <bool FL, bool INV>
+static void cols_r_dispatch(int log_r, unsigned blocks, const NttParams &P, const ColsArgs &a, cudaStream_t st) {
+    switch (log_r) {
+        case 1: k_cols_r<1, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 2: k_cols_r<2, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 3: k_cols_r<3, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 4: k_cols_r<4, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 5: k_cols_r<5, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 6: k_cols_r<6, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 7: k_cols_r<7, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 8: k_cols_r<8, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        default: k_cols_r<9, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+    }
+}
+
+static void launch_cols_r(bool from_limbs, bool inverse, const NttParams &P, const ColsArgs &a, uint64_t vrows,
+                          cudaStream_t st) {
+    const uint64_t ctiles = 1ull << (a.log_s - a.log_r - (12 - a.log_r));
+    const uint64_t nseg = 1ull << (a.log_k - a.log_s);
+    const unsigned blocks = (unsigned)(vrows * kPrimes * nseg * ctiles);
+    const double K = (double)(1ull << a.log_k);
+    const double bytes = from_limbs ? (4.0 * a.Lx * (double)(vrows >> a.coset_bits) + 12.0 * K * (double)vrows)
+                                    : 24.0 * K * (double)vrows;
+    KernelTimed kt(from_limbs ? "ntt_cols_fwd_first" : (inverse ? "ntt_cols_inv" : "ntt_cols_fwd"), bytes);
+    if (from_limbs)
+        cols_r_dispatch<true, false>(a.log_r, blocks, P, a, st);
+    else if (!inverse)
+        cols_r_dispatch<false, false>(a.log_r, blocks, P, a, st);
+    else
+        cols_r_dispatch<false, true>(a.log_r, blocks, P, a, st);
+    count_launch();
+}
+
+template <bool FL>
+static void rows_r_dispatch(int log_c, unsigned blocks, const NttParams &P, const RowsArgs &r, cudaStream_t st) {
+    switch (log_c) {
+        case 9: k_rows_r<9, FL><<<blocks, 32, 0, st>>>(P, r); break;
+        case 10: k_rows_r<10, FL><<<blocks, 64, 0, st>>>(P, r); break;
+        case 11: k_rows_r<11, FL><<<blocks, 128, 0, st>>>(P, r); break;
+        default: k_rows_r<12, FL><<<blocks, 256, 0, st>>>(P, r); break;
+    }
+}
+
 static int tc_for(int log_r, int log_cols) {
     int log_tc = 12 - log_r;
     if (log_tc < 4) log_tc = 4;
@@ -436,17 +659,22 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
 
     if (log_k <= 12) {
         RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_k, bcast ? 1 : 0, square ? 1 : 0, 0};
-        const size_t smem = (size_t)3 * K * 4;
-        set_smem(k_rows<true>, smem);
         KernelTimed kt("ntt_local", 4.0 * N * ((double)La + (square ? 0 : Lb)) + 12.0 * K * N);
-        k_rows<true><<<(unsigned)(N * kPrimes), kThreads, smem, st>>>(P, r);
+        if (log_k >= 9 && !use_radix2()) {
+            rows_r_dispatch<true>(log_k, (unsigned)(N * kPrimes), P, r, st);
+        } else {
+            const size_t smem = (size_t)3 * K * 4;
+            set_smem(k_rows<true>, smem);
+            k_rows<true><<<(unsigned)(N * kPrimes), kThreads, smem, st>>>(P, r);
+        }
         count_launch();
     } else {
         const int log_c = 12;
         const int rest = log_k - log_c;
+        const bool r2 = use_radix2();
         int passes[2];
         int npass;
-        if (rest <= 10) {
+        if (rest <= (r2 ? 10 : 9)) {
             passes[0] = rest;
             npass = 1;
         } else {
@@ -464,25 +692,41 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
             int log_s = log_k;
             for (int ps = 0; ps < npass; ++ps) {
                 ColsArgs a{X, sX, Lx, F, log_k, log_s, passes[ps], 0, cb};
-                a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
-                launch_cols(ps == 0, false, P, a, vrows, st);
+                if (r2) {
+                    a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
+                    launch_cols(ps == 0, false, P, a, vrows, st);
+                } else {
+                    a.log_tc = 12 - passes[ps];
+                    launch_cols_r(ps == 0, false, P, a, vrows, st);
+                }
                 log_s -= passes[ps];
             }
         }
         RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_c, bcast ? 1 : 0, square ? 1 : 0, cb};
-        const size_t smem = (size_t)3 * (1u << log_c) * 4;
-        set_smem(k_rows<false>, smem);
         const uint64_t blocks = VR * kPrimes * (K >> log_c);
-        KernelTimed kt("ntt_rows_fused", 12.0 * (double)K * ((square ? 2.0 : 3.0) * (double)VR));
-        k_rows<false><<<(unsigned)blocks, kThreads, smem, st>>>(P, r);
-        count_launch();
+        {
+            KernelTimed kt("ntt_rows_fused", 12.0 * (double)K * ((square ? 2.0 : 3.0) * (double)VR));
+            if (r2) {
+                const size_t smem = (size_t)3 * (1u << log_c) * 4;
+                set_smem(k_rows<false>, smem);
+                k_rows<false><<<(unsigned)blocks, kThreads, smem, st>>>(P, r);
+            } else {
+                rows_r_dispatch<false>(log_c, (unsigned)blocks, P, r, st);
+            }
+            count_launch();
+        }
         // inverse column passes, innermost first
         int log_s = log_c;
         for (int ps = npass - 1; ps >= 0; --ps) {
             log_s += passes[ps];
             ColsArgs a{nullptr, 0, 0, FA, log_k, log_s, passes[ps], 0, 0};
-            a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
-            launch_cols(false, true, P, a, VR, st);
+            if (r2) {
+                a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
+                launch_cols(false, true, P, a, VR, st);
+            } else {
+                a.log_tc = 12 - passes[ps];
+                launch_cols_r(false, true, P, a, VR, st);
+            }
         }
     }
     CrtArgs c{FA, log_k, C, sC, Lc, (uint32_t)tiles, flags};

@@ -143,5 +143,129 @@ struct CrtConsts {
     uint64_t p0p1;
 };
 
+
+// ---------------------------------------------------------------------------
+// Register-resident radix-2^B stages (all shapes compile-time).
+//
+// A CTA of T threads owns a tile of TC = 2^LOG_TC interleaved transforms of
+// R = 2^LOG_R points each, R * TC = 16 * T: element (position r, transform c)
+// lives at tile index r * TC + c.  In a stage each thread holds 16 elements =
+// 16 / 2^B groups of 2^B points; a group is {base + s*v : v < 2^B} with
+// s = 2^LO, and the stage performs the B radix-2 levels with half-spans
+// s*2^(B-1) .. s (forward, decimation in frequency) or s .. s*2^(B-1)
+// (inverse, decimation in time).  The arithmetic is exactly that of
+// tile_transform; only the grouping of levels changes, so results are
+// identical.  Group id q = t + g*T; transform c = q mod TC; the remaining bits
+// give (low, high) with base = high * s * 2^B + low.
+//
+// Forward stages cover the levels top-down in chunks of 4 (LOG_R = 12:
+// [8..11], [4..7], [0..3]; 9: [5..8], [1..4], [0]); inverse stages walk the
+// same chunks bottom-up, so the last forward and first inverse stage share a
+// thread mapping.
+// ---------------------------------------------------------------------------
+template <int LOG_R, int K>
+struct StageInfo {
+    static constexpr int top = LOG_R - 4 * K;
+    static constexpr int B = top >= 4 ? 4 : top;
+    static constexpr int LO = top - B;
+};
+
+template <int LOG_R>
+struct StagePlan {
+    static constexpr int n = (LOG_R + 3) / 4;
+};
+
+template <int LOG_R, int LOG_TC, int LO, int B>
+struct Stage {
+    static constexpr uint32_t T = 1u << (LOG_R + LOG_TC - 4);
+    __device__ static __forceinline__ void elem(uint32_t t, int j, uint32_t &pos, uint32_t &c) {
+        const int g = j >> B;
+        const uint32_t v = (uint32_t)j & ((1u << B) - 1u);
+        const uint32_t q = t + (uint32_t)g * T;
+        c = q & ((1u << LOG_TC) - 1u);
+        const uint32_t rem = q >> LOG_TC;
+        const uint32_t low = rem & ((1u << LO) - 1u);
+        const uint32_t high = rem >> LO;
+        pos = (high << (LO + B)) + low + (v << LO);
+    }
+    __device__ static __forceinline__ uint32_t addr(uint32_t pos, uint32_t c) {
+        const uint32_t i = (pos << LOG_TC) + c;
+        return i + (i >> 5);   // one pad word per 32 avoids bank conflicts
+    }
+    __device__ static __forceinline__ void store(uint32_t *S, const uint32_t (&x)[16], uint32_t t) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            elem(t, j, pos, c);
+            S[addr(pos, c)] = x[j];
+        }
+    }
+    __device__ static __forceinline__ void load(const uint32_t *S, uint32_t (&x)[16], uint32_t t) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            elem(t, j, pos, c);
+            x[j] = S[addr(pos, c)];
+        }
+    }
+    // tw[e] = w_R^(+/-e), e < R/2
+    template <bool INV>
+    __device__ static __forceinline__ void levels(uint32_t (&x)[16], uint32_t t, const uint32_t *tw, uint32_t p,
+                                                  uint32_t pinv) {
+#pragma unroll
+        for (int step = 0; step < B; ++step) {
+            const int lm = INV ? step : (B - 1 - step);
+            const int mm = 1 << lm;
+            const int lh = LO + lm;
+            const int shift = LOG_R - 1 - lh;
+            const uint32_t hmask = (1u << lh) - 1u;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                if (j & mm) continue;   // partner j + mm stays inside the 2^B group
+                uint32_t pos, c;
+                elem(t, j, pos, c);
+                const uint32_t w = tw[(pos & hmask) << shift];
+                const uint32_t a = x[j];
+                const uint32_t b = x[j + mm];
+                if (!INV) {
+                    x[j] = add_mod(a, b, p);
+                    x[j + mm] = mont_mul(sub_mod(a, b, p), w, p, pinv);
+                } else {
+                    const uint32_t u = mont_mul(b, w, p, pinv);
+                    x[j] = add_mod(a, u, p);
+                    x[j + mm] = sub_mod(a, u, p);
+                }
+            }
+        }
+    }
+};
+
+// Stage number K of the execution order (forward: top-down, inverse: bottom-up).
+template <int LOG_R, int LOG_TC, bool INV, int K>
+struct ExecStage {
+    static constexpr int idx = INV ? (StagePlan<LOG_R>::n - 1 - K) : K;
+    using I = StageInfo<LOG_R, idx>;
+    using S = Stage<LOG_R, LOG_TC, I::LO, I::B>;
+};
+
+// Runs execution stages K .. n-1 on x; S is the shared tile (stage hand-off).
+template <int LOG_R, int LOG_TC, bool INV, int K>
+__device__ __forceinline__ void run_stages(uint32_t (&x)[16], uint32_t *Sm, uint32_t t, const uint32_t *tw,
+                                           uint32_t p, uint32_t pinv) {
+    constexpr int n = StagePlan<LOG_R>::n;
+    if constexpr (K < n) {
+        using Cur = typename ExecStage<LOG_R, LOG_TC, INV, K>::S;
+        if constexpr (K > 0) {
+            using Prev = typename ExecStage<LOG_R, LOG_TC, INV, K - 1>::S;
+            Prev::store(Sm, x, t);
+            __syncthreads();
+            Cur::load(Sm, x, t);
+            __syncthreads();
+        }
+        Cur::template levels<INV>(x, t, tw, p, pinv);
+        run_stages<LOG_R, LOG_TC, INV, K + 1>(x, Sm, t, tw, p, pinv);
+    }
+}
+
 }  // namespace ntt
 }  // namespace gpupi

@@ -10,6 +10,7 @@
 #include "common.cuh"
 #include "batch_arith.h"
 #include "batch_mul_naive.h"
+#include "batch_mul_ntt.h"
 #include "convert_decimal.h"
 #include "pi_engine.h"
 
@@ -724,6 +725,16 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
             uint64_t keep = UINT64_MAX;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
+    // Size the multiply workspace once for the largest product (P * invQ, two
+    // operands of about prec_limbs limbs) so that no level regrows it.
+    {
+        const cudaError_t werr =
+            batch_mp_ensure_workspace(ctx, batch_mul_ntt_workspace_size(1u, prec + 8u, prec + 8u));
+        if (werr != cudaSuccess) {
+            if (own_ctx) batch_mp_destroy(ctx);
+            return werr;
         }
     }
     Profiler prof;
