@@ -4,7 +4,9 @@
 //   * k_school_thread<MA, MB>: one thread per product for operands of at most
 //     MA x MB limbs (the bottom levels of the splitting tree: 3..16-limb rows
 //     in batches of millions).  Register arrays, fully unrolled MACs.
-//   * k_school_cols: one CTA per product, 256 threads x 4 consecutive output
+//   * k_school_warp: one warp per product for L_a + L_b <= 128, eight
+//     products per CTA, carries resolved with one ballot pair.
+//   * k_school_cols: one CTA per product, 64-256 threads x 4 consecutive output
 //     columns.  Each column sum sum_i a_i b_(k-i) is accumulated exactly in a
 //     3-word register with mad.lo.cc / madc.hi.cc / addc (3 instructions per
 //     32x32 product), then the 96-bit column sums are carried into limbs with
@@ -60,10 +62,67 @@ __device__ __forceinline__ void mac3(uint32_t &c0, uint32_t &c1, uint32_t &c2, u
         : "r"(a), "r"(b));
 }
 
-constexpr int kSchoolThreads = 256;
 constexpr int kSchoolV = 4;
-constexpr int kSchoolMaxL = kSchoolThreads * kSchoolV;   // 1024 output limbs
+constexpr int kSchoolMaxL = 256 * kSchoolV;   // 1024 output limbs
 
+// One warp per product, L_a + L_b <= 128: lane l owns output columns
+// 4l .. 4l+3; carries between lanes are resolved with one ballot pair.
+constexpr int kWarpProducts = 8;   // products (warps) per CTA
+
+__global__ void __launch_bounds__(32 * kWarpProducts) k_school_warp(const uint32_t *__restrict__ A,
+                                                                    const uint32_t *__restrict__ B,
+                                                                    uint32_t *__restrict__ C, uint32_t N,
+                                                                    uint32_t La, uint32_t Lb, uint64_t sA,
+                                                                    uint64_t sB, uint64_t sC) {
+    __shared__ uint32_t sa[kWarpProducts][128];
+    __shared__ uint32_t sb[kWarpProducts][128 + 128 + 8];
+    const uint32_t lane = lane_id();
+    const uint32_t w = threadIdx.x >> 5;
+    const uint32_t kPad = La + 4;
+    const uint32_t Lc = La + Lb;
+    for (uint32_t row = blockIdx.x * kWarpProducts + w; row < N; row += gridDim.x * kWarpProducts) {
+        const uint32_t *ar = A + row * sA;
+        const uint32_t *br = B + row * sB;
+        for (uint32_t i = lane; i < La; i += 32) sa[w][i] = ar[i];
+        for (uint32_t j = lane; j < kPad + Lb + 8; j += 32) sb[w][j] = (j >= kPad && j - kPad < Lb) ? br[j - kPad] : 0u;
+        __syncwarp();
+        const uint32_t k0 = lane * kSchoolV;
+        uint32_t c[kSchoolV][3];
+#pragma unroll
+        for (int v = 0; v < kSchoolV; ++v) c[v][0] = c[v][1] = c[v][2] = 0u;
+        if (k0 < Lc) {
+            const int ilo = max(0, (int)k0 + 1 - (int)Lb);
+            const int ihi = min((int)La - 1, (int)k0 + kSchoolV - 1);
+            for (int i = ilo; i <= ihi; ++i) {
+                const uint32_t ai = sa[w][i];
+                const uint32_t *bw = &sb[w][kPad + k0 - i];
+#pragma unroll
+                for (int v = 0; v < kSchoolV; ++v) mac3(c[v][0], c[v][1], c[v][2], ai, bw[v]);
+            }
+        }
+        uint32_t S[kSchoolV + 3];
+        chunk_sum3<kSchoolV>(c, S);
+        uint32_t H[3];
+        H[0] = __shfl_up_sync(0xffffffffu, S[kSchoolV], 1);
+        H[1] = __shfl_up_sync(0xffffffffu, S[kSchoolV + 1], 1);
+        H[2] = __shfl_up_sync(0xffffffffu, S[kSchoolV + 2], 1);
+        if (lane == 0) H[0] = H[1] = H[2] = 0u;
+        uint32_t X[kSchoolV];
+        const uint32_t g = chunk_add_spill<kSchoolV>(S, H, X);
+        bool pp = true;
+#pragma unroll
+        for (int v = 0; v < kSchoolV; ++v) pp = pp && (X[v] == 0xffffffffu);
+        const GroupCarry gc = resolve_group(__ballot_sync(0xffffffffu, g != 0u), __ballot_sync(0xffffffffu, pp), 0u);
+        chunk_increment<kSchoolV>(X, (gc.carry_in_mask >> lane) & 1u);
+        uint32_t *cr = C + row * sC;
+#pragma unroll
+        for (int v = 0; v < kSchoolV; ++v)
+            if (k0 + v < Lc) cr[k0 + v] = X[v];
+        __syncwarp();
+    }
+}
+
+template <int kSchoolThreads>
 __global__ void __launch_bounds__(kSchoolThreads) k_school_cols(const uint32_t *__restrict__ A,
                                                                 const uint32_t *__restrict__ B,
                                                                 uint32_t *__restrict__ C, uint32_t N,
@@ -166,9 +225,19 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
         launch_thread<16, 8>(A, B, C, N, La, Lb, sA, sB, sC, st);
     } else if (La <= 16u && Lb <= 16u) {
         launch_thread<16, 16>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else if (La + Lb <= 128u) {
+        k_school_warp<<<grid_for(N, kWarpProducts, kNumSMs * 32), 32 * kWarpProducts, 0, st>>>(A, B, C, N, La, Lb,
+                                                                                            sA, sB, sC);
+        count_launch();
     } else {
-        k_school_cols<<<grid_for(N, 1, kNumSMs * 16), kSchoolThreads, 0, st>>>(A, B, C, N, La, Lb, sA,
-                                                                             sB, sC);
+        // one CTA per product, 4 output columns per thread
+        const uint32_t g = grid_for(N, 1, kNumSMs * 16);
+        if (La + Lb <= 256u)
+            k_school_cols<64><<<g, 64, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+        else if (La + Lb <= 512u)
+            k_school_cols<128><<<g, 128, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+        else
+            k_school_cols<256><<<g, 256, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
         count_launch();
     }
 }

@@ -36,7 +36,7 @@ def _check_mul(ctx, N, La, Lb, sA, sB, sC, rng, path="auto", extreme=False):
         assert ref.mul_check(N, A, La, sA, B, Lb, sB, got, sC)
 
 
-@pytest.mark.parametrize("La,Lb", [(1, 1), (3, 3), (4, 3), (6, 4), (8, 8), (12, 5), (16, 16), (17, 16),
+@pytest.mark.parametrize("La,Lb", [(1, 1), (3, 3), (4, 3), (6, 4), (8, 8), (12, 5), (16, 16), (17, 16), (21, 16), (64, 64), (65, 64), (150, 50),
                                    (33, 31), (100, 7), (256, 256), (511, 513), (1000, 24)])
 def test_schoolbook(ctx, La, Lb):
     rng = np.random.default_rng(La * 1000 + Lb)
