@@ -61,6 +61,7 @@ _SIGS = [
     ("gpupi_timer_reset", ctypes.c_int, []),
     ("gpupi_timer_report", ctypes.c_size_t, [_p, ctypes.c_size_t]),
     ("gpupi_transfer_bytes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    ("gpupi_mp_add_noalloc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
     ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
 ]
 
@@ -229,6 +230,13 @@ def mul_naive(N, A, La, sA, B, Lb, sB, C, sC):
 def decimal_naive(N, A, L_limb, sA, out, L_dec, s_out):
     _torch()
     _check(lib().gpupi_decimal_naive(N, A, L_limb, sA, out, L_dec, s_out), "batch_decimal_naive")
+
+
+def add_noalloc(N, A, La, sA, B, Lb, sB, C, Lc, sC) -> None:
+    """C = A + B like Context.add, without a context and without any device
+    allocation (gpupi_mp_add_noalloc); for callers that cannot allocate."""
+    _torch()
+    _check(lib().gpupi_mp_add_noalloc(N, A, La, sA, B, Lb, sB, C, Lc, sC), "gpupi_mp_add_noalloc")
 
 
 def launch_count() -> int:

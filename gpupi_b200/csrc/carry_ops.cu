@@ -392,3 +392,78 @@ size_t batch_shift_sub_simple_workspace_size(uint32_t N, uint32_t L_a, uint32_t 
     (void)shift;
     return carry_workspace_bytes(N, L_c);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free batched addition (gpupi_mp_add_noalloc in gpupi_c.h).
+//
+// Some callers cannot allocate device memory at the moment they need an add:
+// code that runs with all device memory already handed to another allocator
+// (a pre-sized pool it must not grow), and latency-critical loops that must
+// not call cudaMalloc/cudaFree because those calls can synchronise the whole
+// device.  For them the per-tile carry flags of long rows live in the fixed
+// array below, compiled into the library, instead of a context workspace.
+//
+// Limit: kNoAllocMaxTiles flag words (256 KiB), i.e. N * ceil(L_c / 4096) tiles
+// for rows on the multi-tile path; larger requests are rejected.
+// The array is shared by every call and keeps the previous call's flags; no
+// word has to start at zero because each tile's CTA writes its flag before
+// the fix-up kernel reads it.  Calls whose kernels overlap on the GPU (two
+// streams, two host threads) would race on the array.
+// ---------------------------------------------------------------------------
+#include "gpupi_c.h"
+
+#include <mutex>
+
+namespace gpupi {
+
+constexpr uint64_t kNoAllocMaxTiles = 65536;
+static __device__ __align__(256) uint32_t g_noalloc_flags[kNoAllocMaxTiles];
+
+// Device address of g_noalloc_flags, looked up once per device (with that
+// device current) on the first call that needs it.
+static uint32_t *g_noalloc_addr[64];
+static std::mutex g_noalloc_mu;
+
+static cudaError_t noalloc_flags_address(uint32_t **out) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void *p = nullptr;
+        err = cudaGetSymbolAddress(&p, g_noalloc_flags);
+        if (err != cudaSuccess) return err;
+        g_noalloc_addr[dev] = static_cast<uint32_t *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return cudaSuccess;
+}
+
+static bool noalloc_view_ok(const uint32_t *d, uint32_t len, uint32_t n, uint32_t stride) {
+    if (n == 0u) return len <= stride;
+    if (d == nullptr) return false;
+    return stride == 0u || len <= stride;
+}
+
+}  // namespace gpupi
+
+extern "C" int gpupi_mp_add_noalloc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
+                                    const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C,
+                                    uint32_t L_c, uint32_t stride_C) {
+    using namespace gpupi;
+    if (!noalloc_view_ok(d_A, L_a, N, stride_A) || !noalloc_view_ok(d_B, L_b, N, stride_B) ||
+        !noalloc_view_ok(d_C, L_c, N, stride_C))
+        return (int)cudaErrorInvalidValue;
+    if (N == 0u || L_c == 0u) return 0;
+    uint32_t *flags = nullptr;
+    if (plan_for(N, L_c) == CarryPlan::Tiles) {
+        const uint64_t tiles = (uint64_t)N * ((L_c + kTileSpan - 1u) / kTileSpan);
+        if (tiles > kNoAllocMaxTiles) return (int)cudaErrorInvalidValue;   // beyond the fixed array
+        const cudaError_t err = noalloc_flags_address(&flags);
+        if (err != cudaSuccess) return (int)err;
+    }
+    GenTwo g{d_A, d_B, L_a, L_b, stride_A, stride_B};
+    run_carry<GenTwo, false>(g, d_C, N, L_c, stride_C, flags);
+    return (int)cudaGetLastError();
+}

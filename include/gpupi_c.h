@@ -110,6 +110,21 @@ size_t gpupi_timer_report(char *buf, size_t cap);
 /* Cumulative host->device and device->host bytes copied by the library. */
 int gpupi_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 
+/* Allocation-free batched addition: C = A + B exactly like gpupi_mp_add, but
+ * without a context and without allocating.  It has no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory when they
+ * need an add (all memory already handed to another allocator, or loops that
+ * must not call cudaMalloc/cudaFree because those can synchronise the device).
+ * The carry flags of long rows live in a fixed 256 KiB array inside the
+ * library: N * ceil(L_c / 4096) must stay <= 65536 when rows take the
+ * multi-tile path (fewer than 9472 rows of more than 4096 limbs), otherwise
+ * the call returns 1 (cudaErrorInvalidValue) and does nothing.  The first
+ * call on each device looks the array up (with that device current); make
+ * that first call before starting any stream capture.  Calls share the
+ * array: two calls whose kernels overlap on the GPU race. */
+int gpupi_mp_add_noalloc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A, const uint32_t *d_B,
+                         uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t L_c, uint32_t stride_C);
+
 /* Multiply crossover: largest L_a + L_b computed by schoolbook (<= 1024). */
 int gpupi_set_mul_crossover(uint32_t max_school_len);
 
