@@ -1,8 +1,8 @@
 // Largest used bit / limb length over a batch (gpupi batch_bitlength.cu:33-245).
 //
-// One warp per row scans down from the top limb, 32 limbs per step, and stops
-// at the first non-zero limb, so a row whose top limb is set costs one 128-byte
-// read instead of a full pass.  Per-CTA maxima meet in one device word; the
+// Few rows: 4096-limb chunks scanned from the top by all CTAs, skipping
+// chunks that cannot beat the best length found so far.  Many rows: one
+// thread per row, bounded by the best length seen so far.  Per-CTA maxima meet in one device word; the
 // last CTA to finish (ticket counter) moves the result straight into pinned,
 // mapped host memory and re-zeroes the word and the counter, so a call is one
 // launch plus one stream synchronisation — no memset, no device-to-host copy.
@@ -16,34 +16,98 @@
 
 namespace gpupi {
 
+// Few (long) rows: the rows are cut into 4096-limb chunks counted from the
+// top; work item w = (chunk c, row) with c major, so the first wave of CTAs
+// reads the top chunk of every row.  A chunk is skipped when even its top
+// limb could not beat the best length already published in dev_max, so a
+// call usually reads one wave of chunks however long the zero run above the
+// highest set limb is.
+constexpr uint32_t kChunk = 4096;   // 256 threads x 16 limbs
+
 template <bool BITS>
-__global__ void __launch_bounds__(256) length_max_kernel(const uint32_t *__restrict__ A, uint32_t N, uint32_t L,
-                                                         uint64_t stride, uint32_t *dev_max, uint32_t *dev_count,
-                                                         volatile uint32_t *host_out) {
+__global__ void __launch_bounds__(256) length_max_chunks_kernel(const uint32_t *__restrict__ A, uint32_t N,
+                                                                uint32_t L, uint64_t stride, uint64_t items,
+                                                                uint32_t *dev_max, uint32_t *dev_count,
+                                                                volatile uint32_t *host_out) {
+    __shared__ uint32_t cta_max;
+    __shared__ bool last;
+    __shared__ bool skip;
+    for (uint64_t w = blockIdx.x; w < items; w += gridDim.x) {
+        const uint32_t row = (uint32_t)(w % N);
+        const uint64_t c = w / N;
+        const int64_t hi = (int64_t)L - (int64_t)(c * kChunk);   // chunk covers [hi - 4096, hi)
+        if (threadIdx.x == 0) {
+            const uint32_t cur = *((volatile uint32_t *)dev_max);
+            const uint64_t best_possible = BITS ? (uint64_t)hi * 32u : (uint64_t)hi;
+            skip = best_possible <= cur;
+            cta_max = 0u;
+        }
+        __syncthreads();
+        if (!skip) {
+            const uint32_t *a = A + row * stride;
+            uint32_t best = 0u;
+#pragma unroll 4
+            for (int k = 0; k < 16; ++k) {
+                // k-th 256-limb slab from the top of the chunk, coalesced across the CTA
+                const int64_t j = hi - 1 - (int64_t)k * 256 - (int64_t)threadIdx.x;
+                if (j >= 0 && j > hi - 1 - (int64_t)kChunk) {
+                    const uint32_t v = a[j];
+                    if (v != 0u) {
+                        const uint32_t len = BITS ? (uint32_t)j * 32u + (32u - __clz(v)) : (uint32_t)j + 1u;
+                        best = max(best, len);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (lane_id() == 0 && best) atomicMax(&cta_max, best);
+            __syncthreads();
+            if (threadIdx.x == 0 && cta_max) atomicMax(dev_max, cta_max);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t ticket = atomicAdd(dev_count, 1u);
+        last = (ticket == gridDim.x - 1u);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t v = atomicExch(dev_max, 0u);
+        *host_out = v;
+        __threadfence_system();
+        atomicExch(dev_count, 0u);
+    }
+}
+
+// Many rows: one thread per row, reading down from the top limb only while
+// the row could still beat the longest length this thread has seen (after
+// the first row that is usually a single 4-byte read per row).
+template <bool BITS>
+__global__ void __launch_bounds__(256) length_max_rows_kernel(const uint32_t *__restrict__ A, uint32_t N,
+                                                              uint32_t L, uint64_t stride, uint32_t *dev_max,
+                                                              uint32_t *dev_count, volatile uint32_t *host_out) {
     __shared__ uint32_t cta_max;
     __shared__ bool last;
     if (threadIdx.x == 0) cta_max = 0u;
     __syncthreads();
-    const uint32_t lane = lane_id();
-    const uint32_t wpc = blockDim.x >> 5;
     uint32_t best = 0u;
-    for (uint32_t row = blockIdx.x * wpc + (threadIdx.x >> 5); row < N; row += gridDim.x * wpc) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < N; row += gridDim.x * blockDim.x) {
         const uint32_t *a = A + row * stride;
-        for (int64_t top = (int64_t)L - 1; top >= 0; top -= 32) {
-            const int64_t j = top - lane;
-            const uint32_t v = (j >= 0) ? a[j] : 0u;
-            const uint32_t nz = __ballot_sync(0xffffffffu, v != 0u);
-            if (nz != 0u) {
-                const uint32_t hl = (uint32_t)(__ffs(nz) - 1);   // lowest lane = highest limb
-                const uint32_t limb = (uint32_t)(top - hl);
-                const uint32_t topv = __shfl_sync(0xffffffffu, v, hl);
-                const uint32_t len = BITS ? limb * 32u + (32u - __clz(topv)) : limb + 1u;
+        const int64_t floor_limb = BITS ? (int64_t)(best >> 5) : (int64_t)best;
+        for (int64_t j = (int64_t)L - 1; j >= floor_limb; --j) {
+            const uint32_t v = a[j];
+            if (v != 0u) {
+                const uint32_t len = BITS ? (uint32_t)j * 32u + (32u - __clz(v)) : (uint32_t)j + 1u;
                 best = max(best, len);
                 break;
             }
         }
     }
-    if (lane == 0 && best) atomicMax(&cta_max, best);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane_id() == 0 && best) atomicMax(&cta_max, best);
     __syncthreads();
     if (threadIdx.x == 0) {
         if (cta_max) atomicMax(dev_max, cta_max);
@@ -107,8 +171,14 @@ static uint32_t length_max(const uint32_t *A, uint32_t *workspace, uint32_t N, u
     if (!s) return 0u;
     cudaStream_t st = current_stream();
     *s->host = 0xffffffffu;
-    length_max_kernel<BITS><<<grid_for(N, 8, kNumSMs * 8), 256, 0, st>>>(A, N, L, stride, s->dev, s->dev + 1,
-                                                                        s->host_dev);
+    if (N >= 4096u)
+        length_max_rows_kernel<BITS><<<grid_for(N, 256, kNumSMs * 8), 256, 0, st>>>(A, N, L, stride, s->dev,
+                                                                                  s->dev + 1, s->host_dev);
+    else {
+        const uint64_t items = (uint64_t)N * ((L + kChunk - 1u) / kChunk);
+        length_max_chunks_kernel<BITS><<<grid_for(items, 1, kNumSMs * 8), 256, 0, st>>>(
+            A, N, L, stride, items, s->dev, s->dev + 1, s->host_dev);
+    }
     count_launch();
     cudaStreamSynchronize(st);
     note_d2h(sizeof(uint32_t));

@@ -283,8 +283,11 @@ static void run_carry(const Gen &gen, uint32_t *C, uint32_t N, uint32_t Lc, uint
         const unsigned warps = 8;
         if (Lc <= 64u) {
             carry_warp_rows<Gen, SUB, 2><<<grid_for(N, warps), warps * 32, 0, st>>>(gen, C, sC, N, Lc);
-        } else {
+        } else if (Lc <= 1024u) {
             carry_warp_rows<Gen, SUB, 4><<<grid_for(N, warps), warps * 32, 0, st>>>(gen, C, sC, N, Lc);
+        } else {
+            // long rows: more 32-limb groups in flight per warp
+            carry_warp_rows<Gen, SUB, 8><<<grid_for(N, warps), warps * 32, 0, st>>>(gen, C, sC, N, Lc);
         }
         GPUPI_LAUNCH_CHECK();
     } else {

@@ -463,6 +463,18 @@ __device__ __forceinline__ void crt_chunk(const NttParams &P, const uint32_t *F0
                                           uint32_t Lc, int64_t base, uint32_t (&S)[kCrtV + 3]) {
     uint32_t c[kCrtV][3];
     const uint64_t span = COSET ? 2 * K : K;
+    if (!COSET && base >= 0 && (uint64_t)base + kCrtV <= K && base + kCrtV <= (int64_t)Lc) {
+        // whole chunk inside the row: one 128-bit load per prime (K and base are multiples of 4)
+        const uint4 r0 = *reinterpret_cast<const uint4 *>(F0 + base);
+        const uint4 r1 = *reinterpret_cast<const uint4 *>(F0 + K + base);
+        const uint4 r2 = *reinterpret_cast<const uint4 *>(F0 + 2 * K + base);
+        garner(P, r0.x, r1.x, r2.x, c[0]);
+        garner(P, r0.y, r1.y, r2.y, c[1]);
+        garner(P, r0.z, r1.z, r2.z, c[2]);
+        garner(P, r0.w, r1.w, r2.w, c[3]);
+        chunk_sum3<kCrtV>(c, S);
+        return;
+    }
 #pragma unroll
     for (int v = 0; v < kCrtV; ++v) {
         const int64_t i = base + v;
