@@ -1,28 +1,34 @@
 // Batched exact multiplication by three-prime NTT (gpupi batch_mul_ntt.cu;
 // API batch_mul_ntt.h:24-40).
 //
-// Per product row, per prime q, the workspace holds a transform of K = 2^k
-// points (K >= L_a + L_b - 1, so the cyclic convolution has no wrap).
-// Layout: F[row][q][K] (u32, plain residues).  A and B each get one such
-// array (FA, FB); B is transformed once when it is broadcast (stride 0) and
-// not at all when B is A (squaring).
+// Shape.  A product of L_c = L_a + L_b limbs is a cyclic convolution of
+// M * K points, K = 2^k <= 2^25, M <= 8, M * K >= L_a + L_b - 1.  M = 1 for
+// products up to 2^25 points.  Longer products are split into M cosets:
+// with c_i = g^(iK) (g a generator, i < M) the residues
+// C_i = A B mod (x^K - c_i) are K-point cyclic convolutions of the twisted
+// inputs (A mod (x^K - c_i))(g^i x), and the M blocks of K coefficients of
+// C = A B follow from C_i = sum_b C_b c_i^b by the inverse Vandermonde
+// matrix of the nodes c_i.
 //
-// Pass structure (four-step decomposition K = R1 * [R2 *] C, C <= 4096):
-//   k_cols<limbs,fwd>   load limbs, reduce mod p, R1-point DIF down each
-//                       column of a [R1][TC] shared tile, twist by w_K^(c*k1),
-//                       store                               (strided, coalesced in c)
-//   k_cols<ws,fwd>      same on each segment for R2 (3-pass sizes only)
-//   k_rows              C-point DIF of the A and B segments, pointwise
-//                       product * K^-1, C-point inverse DIT, store   (contiguous)
-//   k_cols<ws,inv>      untwist + inverse DIT on columns, mirror order
-//   k_crt               Garner CRT to 96-bit coefficients, carry to limbs
-//                       (+ carry_fixup_kernel when a row spans several tiles)
-// Small products (K <= 4096) are one k_rows<from limbs> launch + k_crt.
-// Products longer than 2^27 limbs (up to 2^28) use two cosets of 2^27
-// points (see coef_residue), the third prime's 2-adicity being 27.
+// Workspace: F[vrow][q][K] residues (vrow = row * M + coset), one such array
+// for A (FA) and one for B (FB; none when B is A, one row when B is
+// broadcast), then the CRT tile flags.
 //
-// The shared-memory butterflies are radix-2 levels separated by
-// __syncthreads; every DIF level needs one Montgomery product per pair.
+// Passes (four-step decomposition K = R1 [* R2] * C, C = 4096):
+//   k_cols_r<first>   load limbs (fold + twist for cosets), R1-point DIF
+//                     down each column of a 4096-residue tile, twist by
+//                     w_K^(col * bitrev(pos)), store
+//   k_cols_r          same on each segment for R2 (sizes above 2^21)
+//   k_rows_r          C-point DIF of the A and B segments, pointwise product
+//                     * K^-1, C-point inverse DIT, store
+//   k_cols_r<inv>     untwist + inverse DIT on columns, mirror order
+//   k_combine<M>      (M > 1) untwist the cosets, inverse Vandermonde
+//   k_crt             Garner CRT to 96-bit coefficients, carry into limbs
+//                     (+ carry_fixup_kernel when a row spans several tiles)
+// Small products (K <= 4096) are one k_rows_r (or k_rows_small) launch and
+// k_crt.  Every CTA handles one prime, fixed at compile time inside the CTA;
+// the prime is the slowest grid index, so an SM works on one prime's tables
+// and code at a time.
 #include "ntt_core.cuh"
 #include "carry_tile.cuh"
 #include "batch_mul_ntt.h"
@@ -34,21 +40,15 @@
 namespace gpupi {
 namespace ntt {
 
-static const uint32_t kP[kPrimes] = {3221225473u, 3489660929u, 3892314113u};
-static const uint32_t kGen[kPrimes] = {5u, 3u, 3u};   // primitive roots
+static const uint32_t kP[kPrimes] = {Prime<0>::p, Prime<1>::p, Prime<2>::p};
+static const uint32_t kGen[kPrimes] = {Prime<0>::g, Prime<1>::g, Prime<2>::g};
 
 struct NttParams {
-    PrimeConsts pr[kPrimes];
-    CrtConsts crt;
     Tables tab;
-    // two-coset split of a 2^28-point product: c1 = beta^(2^27) and
-    // (c1 - 1)^-1, both Montgomery form, per prime
-    uint32_t coset_c[kPrimes];
-    uint32_t coset_cm1_inv[kPrimes];
 };
 
 // ---------------------------------------------------------------------------
-// Host modular helpers (table construction)
+// Host modular helpers (table construction, coset matrices)
 // ---------------------------------------------------------------------------
 static uint32_t h_mul(uint32_t a, uint32_t b, uint32_t p) { return (uint32_t)((uint64_t)a * b % p); }
 static uint32_t h_pow(uint32_t a, uint64_t e, uint32_t p) {
@@ -63,35 +63,17 @@ static uint32_t h_pow(uint32_t a, uint64_t e, uint32_t p) {
 }
 static uint32_t h_inv(uint32_t a, uint32_t p) { return h_pow(a, p - 2u, p); }
 static uint32_t h_mont(uint32_t x, uint32_t p) { return (uint32_t)(((uint64_t)x << 32) % p); }
-static uint32_t h_inv_2_32(uint32_t p) {
-    uint32_t x = p;
-    for (int i = 0; i < 5; ++i) x *= 2u - p * x;
-    return x;
-}
 
 static NttParams make_params(const NTTPrecomputedTables &t) {
     NttParams P{};
-    for (int q = 0; q < kPrimes; ++q) {
-        P.pr[q].p = kP[q];
-        P.pr[q].pinv = h_inv_2_32(kP[q]);
-    }
-    P.crt.p0_inv_mod_p1_m = h_mont(h_inv(kP[0] % kP[1], kP[1]), kP[1]);
-    P.crt.p0_inv_mod_p2_m = h_mont(h_inv(kP[0] % kP[2], kP[2]), kP[2]);
-    P.crt.p1_inv_mod_p2_m = h_mont(h_inv(kP[1] % kP[2], kP[2]), kP[2]);
-    P.crt.p0p1 = (uint64_t)kP[0] * kP[1];
     const uint32_t *lv1 = reinterpret_cast<const uint32_t *>(t.roots_table_lv1);
     const uint32_t *lv2 = reinterpret_cast<const uint32_t *>(t.roots_table_lv2);
-    P.tab.tw_lo = lv1;
-    P.tab.tw_hi = lv2;
-    P.tab.beta_lo = lv2 + 2 * kPrimes * kHiSize;
-    P.tab.beta_hi = P.tab.beta_lo + 2 * kPrimes * kLoSize;
+    P.tab.root_lo = reinterpret_cast<const uint2 *>(lv1);
+    P.tab.root_hi = reinterpret_cast<const uint2 *>(lv1 + kRootLoWords);
+    P.tab.level = reinterpret_cast<const uint2 *>(lv1 + kLevelOffset);
+    P.tab.coset_lo = lv2;
+    P.tab.coset_hi = lv2 + kCosetWords;
     P.tab.inv2n = reinterpret_cast<const uint32_t *>(t.inv2n_table);
-    for (int q = 0; q < kPrimes; ++q) {
-        const uint32_t c1 = h_pow(kGen[q], 1ull << kMaxLog, kP[q]);
-        P.coset_c[q] = h_mont(c1, kP[q]);
-        const uint32_t cm1 = (c1 == 0u) ? kP[q] - 1u : c1 - 1u;   // c1 - 1 mod p without 32-bit overflow
-        P.coset_cm1_inv[q] = h_mont(h_inv(cm1, kP[q]), kP[q]);
-    }
     return P;
 }
 
@@ -99,95 +81,161 @@ static NttParams make_params(const NTTPrecomputedTables &t) {
 // Kernels
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
+constexpr int kTile = 4096;                    // residues per register-stage CTA tile
+constexpr int kTilePad = kTile + kTile / 32;   // padded shared-memory words
 
-// Per-prime constants chosen by value (indexing the kernel-parameter arrays
-// with a run-time prime index would force a local-memory copy).
-__device__ __forceinline__ PrimeConsts prime_of(const NttParams &P, int q) {
-    return q == 0 ? P.pr[0] : (q == 1 ? P.pr[1] : P.pr[2]);
-}
-__device__ __forceinline__ uint32_t sel3(const uint32_t (&v)[kPrimes], int q) {
-    return q == 0 ? v[0] : (q == 1 ? v[1] : v[2]);
+// Grid index -> (prime, index within that prime's third of the grid).
+__device__ __forceinline__ int grid_prime(uint64_t &b) {
+    const uint32_t per = gridDim.x / kPrimes;
+    const int q = (int)(blockIdx.x / per);
+    b = blockIdx.x - (uint32_t)q * per;
+    return q;
 }
 
 struct ColsArgs {
     const uint32_t *X;   // limbs (first forward pass only)
     uint64_t sX;
     uint32_t Lx;
+    uint32_t nb;         // K-limb blocks of X folded into each coset (first pass)
     uint32_t *F;         // workspace of this operand: F[vrow][q][K]
-    int log_k, log_s, log_r, log_tc;
-    int coset_bits;      // 1: vrow = 2*row + coset (2^28-point products)
+    int log_k, log_s;
+    int M;               // cosets per row
 };
 
-template <bool FROM_LIMBS, bool INVERSE>
-__global__ void __launch_bounds__(kThreads) k_cols(NttParams P, ColsArgs a) {
-    extern __shared__ uint32_t smem[];
-    const uint32_t R = 1u << a.log_r;
-    const uint32_t TC = 1u << a.log_tc;
-    uint32_t *T = smem;
-    uint32_t *tw = smem + R * TC;
-    const int log_cols = a.log_s - a.log_r;
-    const uint32_t ctiles = 1u << (log_cols - a.log_tc);
+// Residue q of element i (natural order) of coset `coset` of operand row xr:
+// (X mod (x^K - c)) [i] * g^(coset * i), c = g^(coset K) (Montgomery form cm).
+template <int Q>
+__device__ __forceinline__ uint32_t load_operand(const ColsArgs &a, const uint32_t *xr, uint64_t i, uint64_t K,
+                                                 int coset, uint32_t cm, const uint32_t *clo,
+                                                 const uint32_t *chi) {
+    if (a.M == 1) return (i < a.Lx) ? reduce_limb<Q>(__ldg(xr + i)) : 0u;
+    uint32_t acc = 0u;
+    for (int b = (int)a.nb - 1; b >= 0; --b) {   // Horner over the K-limb blocks
+        const uint64_t ii = i + (uint64_t)b * K;
+        const uint32_t xv = (ii < a.Lx) ? reduce_limb<Q>(__ldg(xr + ii)) : 0u;
+        acc = add_n<Q>(coset ? norm<Q>(mont<Q>(acc, cm)) : acc, xv);
+    }
+    return coset ? mul_coset<Q>(acc, clo, chi, (uint32_t)coset * (uint32_t)i) : acc;
+}
+
+// Offset of element j from element 0 in a LO = 0 stage with 2^B-point groups
+// (LOG_R >= 4): j = g 2^B + v sits at pos_0 + v + g 2^(LOG_R - 4 + B), bits
+// disjoint from those of pos_0.
+__host__ __device__ constexpr uint32_t stage_delta(int j, int B, int log_r) {
+    return ((uint32_t)j & ((1u << B) - 1u)) + (((uint32_t)j >> B) << (log_r - 4 + B));
+}
+
+// Twist the 16 residues of stage S (the LO = 0 stage: last forward, first
+// inverse) by w_S^(col * bitrev(pos)) or its inverse, E = colsh * bitrev(pos)
+// with colsh = col << shift.  For LOG_R >= 4 the column is the same for all
+// 16 residues and bitrev(pos_j) = bitrev(pos_0) + sum over the set bits i of
+// j of bitrev(delta_(2^i)), so the 16 factors are the subset products of
+// w^(E_0) and four D_i = w^(colsh bitrev(delta_(2^i))): five table lookups
+// and fifteen products instead of sixteen scattered lookup pairs.
+template <class S, int LOG_R, int Q>
+__device__ __forceinline__ void twist16(uint32_t (&x)[16], uint32_t t, uint32_t c0, int shift, const uint2 *lo,
+                                        const uint2 *hi) {
+    if constexpr (LOG_R >= 4) {
+        constexpr int B = S::kB;
+        static_assert(S::kLO == 0, "twist stage");
+        uint32_t pos0, c;
+        S::elem(t, 0, pos0, c);
+        const uint32_t colsh = (c0 + c) << shift;
+        uint32_t F[16];
+        F[0] = root_m<Q>(lo, hi, colsh * bitrev(pos0, LOG_R));
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t D = root_m<Q>(lo, hi, colsh * crev(stage_delta(1 << i, B, LOG_R), LOG_R));
+#pragma unroll
+            for (int k = 0; k < (1 << i); ++k) F[(1 << i) + k] = mont<Q>(F[k], D);   // lazy, < 2p
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(x[j], F[j]));
+    } else {
+        // short columns: the 16 residues span several columns
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            S::elem(t, j, pos, c);
+            x[j] = mul_root<Q>(x[j], lo, hi, ((c0 + c) << shift) * bitrev(pos, LOG_R));
+        }
+    }
+}
+
+// Column pass: R = 2^LOG_R (<= 512) points per column, TC = 4096 / R columns
+// per CTA; segment of S = 2^log_s points viewed as [R][S/R].
+template <int LOG_R, bool FROM_LIMBS, bool INVERSE, int Q>
+__device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a, uint64_t b, uint32_t *Sm,
+                                          uint2 *tw) {
+    constexpr int LOG_TC = 12 - LOG_R;
+    constexpr int NS = StagePlan<LOG_R>::n;
+    using First = typename ExecStage<LOG_R, LOG_TC, INVERSE, 0>::S;
+    using Last = typename ExecStage<LOG_R, LOG_TC, INVERSE, NS - 1>::S;
+    const int log_cols = a.log_s - LOG_R;
+    const uint32_t ctiles = 1u << (log_cols - LOG_TC);
     const uint32_t nseg = 1u << (a.log_k - a.log_s);
-    uint64_t b = blockIdx.x;
-    const int q = (int)(b % kPrimes);
-    b /= kPrimes;
     const uint32_t ct = (uint32_t)(b % ctiles);
     b /= ctiles;
     const uint32_t seg = (uint32_t)(b % nseg);
     const uint64_t vrow = b / nseg;
-    const PrimeConsts pc = prime_of(P, q);
-    const uint32_t p = pc.p, pinv = pc.pinv;
     const int dir = INVERSE ? 1 : 0;
     const uint64_t K = 1ull << a.log_k;
-    const uint32_t *twhi = tw_hi_ptr(P.tab, dir, q);
-    const uint32_t *twlo = tw_lo_ptr(P.tab, dir, q);
-    for (uint32_t e = threadIdx.x; e < R / 2; e += blockDim.x) tw[e] = __ldg(twhi + (e << (13 - a.log_r)));
-    uint32_t *F = a.F + vrow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << a.log_s);
-    const uint32_t c0 = ct << a.log_tc;
+    const uint2 *twhi = root_hi_ptr(P.tab, dir, Q);
+    const uint2 *twlo = root_lo_ptr(P.tab, dir, Q);
+    const uint2 *lev = level_ptr(P.tab, dir, Q);
+    for (uint32_t e = threadIdx.x; e < (1u << LOG_R) - 1u; e += kThreads) tw[e] = __ldg(lev + e);
+    uint32_t *F = a.F + vrow * 3 * K + (uint64_t)Q * K + ((uint64_t)seg << a.log_s);
+    const uint32_t c0 = ct << LOG_TC;
     const int twist_shift = kMaxLog - a.log_s;
-    for (uint32_t idx = threadIdx.x; idx < R * TC; idx += blockDim.x) {
-        const uint32_t r = idx >> a.log_tc;
-        const uint32_t c = idx & (TC - 1u);
-        const uint64_t i = ((uint64_t)r << log_cols) + c0 + c;
-        uint32_t v;
-        if (FROM_LIMBS) {
-            const uint64_t row = vrow >> a.coset_bits;
-            const uint32_t *xr = a.X + row * a.sX;
-            v = (i < a.Lx) ? reduce_limb(xr[i], p) : 0u;
-            if (a.coset_bits) {
-                // a mod (x^K - c_j) = a_low + c_j * a_high, then scale by beta_j^i
-                const uint64_t i2 = i + K;
-                const uint32_t hi = (i2 < a.Lx) ? reduce_limb(xr[i2], p) : 0u;
-                if ((vrow & 1u) == 0u) {
-                    v = add_mod(v, hi, p);
-                } else {
-                    v = add_mod(v, mont_mul(hi, sel3(P.coset_c, q), p, pinv), p);
-                    v = mont_mul(v, root_pow(beta_lo_ptr(P.tab, 0, q), beta_hi_ptr(P.tab, 0, q), (uint32_t)i, p, pinv),
-                                 p, pinv);
-                }
-            }
-        } else {
-            v = F[i];
+    const uint32_t t = threadIdx.x;
+    uint32_t x[16];
+    if constexpr (FROM_LIMBS) {
+        const uint64_t row = vrow / (uint32_t)a.M;
+        const int coset = (int)(vrow - row * (uint32_t)a.M);
+        const uint32_t *xr = a.X + row * a.sX;
+        const uint32_t *clo = coset_lo_ptr(P.tab, 0, Q);
+        const uint32_t *chi = coset_hi_ptr(P.tab, 0, Q);
+        // coset node c = g^(coset K), Montgomery form
+        const uint32_t cm = (a.M > 1) ? mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << a.log_k) : 0u;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+            x[j] = load_operand<Q>(a, xr, i, K, coset, cm, clo, chi);
         }
-        if (INVERSE) {
-            const uint32_t E = ((c0 + c) * bitrev(r, a.log_r)) << twist_shift;
-            v = mont_mul(v, root_pow(twlo, twhi, E, p, pinv), p, pinv);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            x[j] = F[((uint64_t)pos << log_cols) + c0 + c];
         }
-        T[idx] = v;
+        if constexpr (INVERSE) twist16<First, LOG_R, Q>(x, t, c0, twist_shift, twlo, twhi);
     }
-    __syncthreads();
-    tile_transform<INVERSE>(T, a.log_r, a.log_tc, tw, p, pinv);
-    for (uint32_t idx = threadIdx.x; idx < R * TC; idx += blockDim.x) {
-        const uint32_t r = idx >> a.log_tc;
-        const uint32_t c = idx & (TC - 1u);
-        const uint64_t i = ((uint64_t)r << log_cols) + c0 + c;
-        uint32_t v = T[idx];
-        if (!INVERSE) {
-            const uint32_t E = ((c0 + c) * bitrev(r, a.log_r)) << twist_shift;
-            v = mont_mul(v, root_pow(twlo, twhi, E, p, pinv), p, pinv);
-        }
-        F[i] = v;
+    __syncthreads();   // twiddle table ready
+    run_stages<LOG_R, LOG_TC, INVERSE, Q, 0>(x, Sm, t, tw);
+    if constexpr (!INVERSE) twist16<Last, LOG_R, Q>(x, t, c0, twist_shift, twlo, twhi);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t pos, c;
+        Last::elem(t, j, pos, c);
+        F[((uint64_t)pos << log_cols) + c0 + c] = x[j];
     }
+}
+
+template <int LOG_R, bool FROM_LIMBS, bool INVERSE>
+__global__ void __launch_bounds__(kThreads) k_cols_r(NttParams P, ColsArgs a) {
+    __shared__ uint32_t Sm[kTilePad];
+    __shared__ uint2 tw[(1 << LOG_R) - 1];
+    uint64_t b;
+    const int q = grid_prime(b);
+    if (q == 0)
+        cols_body<LOG_R, FROM_LIMBS, INVERSE, 0>(P, a, b, Sm, tw);
+    else if (q == 1)
+        cols_body<LOG_R, FROM_LIMBS, INVERSE, 1>(P, a, b, Sm, tw);
+    else
+        cols_body<LOG_R, FROM_LIMBS, INVERSE, 2>(P, a, b, Sm, tw);
 }
 
 struct RowsArgs {
@@ -199,182 +247,37 @@ struct RowsArgs {
     uint32_t Lb;
     uint32_t *FA;
     const uint32_t *FB;
-    int log_k, log_c;
+    int log_k;
+    int M;               // cosets per row
     int b_bcast;         // B row 0 serves every row
     int square;          // B is A
-    int coset_bits;      // virtual rows are (row, coset) pairs
 };
-
-template <bool FROM_LIMBS>
-__global__ void __launch_bounds__(kThreads) k_rows(NttParams P, RowsArgs a) {
-    extern __shared__ uint32_t smem[];
-    const uint32_t C = 1u << a.log_c;
-    uint32_t *SA = smem;
-    uint32_t *SB = smem + C;
-    uint32_t *twf = smem + 2 * C;
-    uint32_t *twi = twf + C / 2;
-    uint64_t b = blockIdx.x;
-    const int q = (int)(b % kPrimes);
-    b /= kPrimes;
-    const uint32_t nseg = 1u << (a.log_k - a.log_c);
-    const uint32_t seg = (uint32_t)(b % nseg);
-    const uint64_t vrow = b / nseg;
-    const uint64_t brow = a.b_bcast ? (vrow & ((1u << a.coset_bits) - 1u)) : vrow;
-    const PrimeConsts pc = prime_of(P, q);
-    const uint32_t p = pc.p, pinv = pc.pinv;
-    const uint64_t K = 1ull << a.log_k;
-    const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + q);
-    const uint32_t *thf = tw_hi_ptr(P.tab, 0, q);
-    const uint32_t *thi = tw_hi_ptr(P.tab, 1, q);
-    for (uint32_t e = threadIdx.x; e < C / 2; e += blockDim.x) {
-        twf[e] = __ldg(thf + (e << (13 - a.log_c)));
-        twi[e] = __ldg(thi + (e << (13 - a.log_c)));
-    }
-    const uint64_t offA = vrow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << a.log_c);
-    const uint64_t offB = brow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << a.log_c);
-    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-        if (FROM_LIMBS) {
-            SA[i] = (i < a.La) ? reduce_limb(a.A[vrow * a.sA + i], p) : 0u;
-            if (!a.square) SB[i] = (i < a.Lb) ? reduce_limb(a.B[brow * a.sB + i], p) : 0u;
-        } else {
-            SA[i] = a.FA[offA + i];
-            if (!a.square) SB[i] = a.FB[offB + i];
-        }
-    }
-    __syncthreads();
-    tile_transform<false>(SA, a.log_c, 0, twf, p, pinv);
-    if (!a.square) tile_transform<false>(SB, a.log_c, 0, twf, p, pinv);
-    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) {
-        const uint32_t x = SA[i];
-        const uint32_t y = a.square ? x : SB[i];
-        SA[i] = mont_mul(mont_mul(x, y, p, pinv), scale, p, pinv);
-    }
-    __syncthreads();
-    tile_transform<true>(SA, a.log_c, 0, twi, p, pinv);
-    for (uint32_t i = threadIdx.x; i < C; i += blockDim.x) a.FA[offA + i] = SA[i];
-}
-
-// ---------------------------------------------------------------------------
-// Register-stage kernels (ntt_core.cuh: Stage / run_stages).  Same arithmetic
-// as k_cols / k_rows, with 16 residues per thread and shared memory touched
-// only between stages of up to four radix-2 levels.
-// ---------------------------------------------------------------------------
-constexpr int kTile = 4096;                    // elements per register-stage CTA tile
-constexpr int kTilePad = kTile + kTile / 32;   // padded shared-memory words
-
-__device__ __forceinline__ uint32_t load_operand(const NttParams &P, const ColsArgs &a, const uint32_t *F,
-                                                 uint64_t vrow, uint64_t i, uint64_t K, int q, uint32_t p,
-                                                 uint32_t pinv) {
-    (void)F;
-    const uint64_t row = vrow >> a.coset_bits;
-    const uint32_t *xr = a.X + row * a.sX;
-    uint32_t v = (i < a.Lx) ? reduce_limb(xr[i], p) : 0u;
-    if (a.coset_bits) {
-        // a mod (x^K - c_j) = a_low + c_j * a_high, then scale by beta_j^i
-        const uint64_t i2 = i + K;
-        const uint32_t hi = (i2 < a.Lx) ? reduce_limb(xr[i2], p) : 0u;
-        if ((vrow & 1u) == 0u) {
-            v = add_mod(v, hi, p);
-        } else {
-            v = add_mod(v, mont_mul(hi, sel3(P.coset_c, q), p, pinv), p);
-            v = mont_mul(v, root_pow(beta_lo_ptr(P.tab, 0, q), beta_hi_ptr(P.tab, 0, q), (uint32_t)i, p, pinv), p,
-                         pinv);
-        }
-    }
-    return v;
-}
-
-// Column pass: R = 2^LOG_R (<= 512) points per column, TC = 4096 / R columns.
-template <int LOG_R, bool FROM_LIMBS, bool INVERSE>
-__global__ void __launch_bounds__(kThreads) k_cols_r(NttParams P, ColsArgs a) {
-    constexpr int LOG_TC = 12 - LOG_R;
-    constexpr int NS = StagePlan<LOG_R>::n;
-    using First = typename ExecStage<LOG_R, LOG_TC, INVERSE, 0>::S;
-    using Last = typename ExecStage<LOG_R, LOG_TC, INVERSE, NS - 1>::S;
-    __shared__ uint32_t Sm[kTilePad];
-    __shared__ uint32_t tw[(1 << LOG_R) / 2 > 0 ? (1 << LOG_R) / 2 : 1];
-    const int log_cols = a.log_s - LOG_R;
-    const uint32_t ctiles = 1u << (log_cols - LOG_TC);
-    const uint32_t nseg = 1u << (a.log_k - a.log_s);
-    uint64_t b = blockIdx.x;
-    const int q = (int)(b % kPrimes);
-    b /= kPrimes;
-    const uint32_t ct = (uint32_t)(b % ctiles);
-    b /= ctiles;
-    const uint32_t seg = (uint32_t)(b % nseg);
-    const uint64_t vrow = b / nseg;
-    const PrimeConsts pc = prime_of(P, q);
-    const uint32_t p = pc.p, pinv = pc.pinv;
-    const int dir = INVERSE ? 1 : 0;
-    const uint64_t K = 1ull << a.log_k;
-    const uint32_t *twhi = tw_hi_ptr(P.tab, dir, q);
-    const uint32_t *twlo = tw_lo_ptr(P.tab, dir, q);
-    for (uint32_t e = threadIdx.x; e < (1u << LOG_R) / 2; e += kThreads) tw[e] = __ldg(twhi + (e << (13 - LOG_R)));
-    uint32_t *F = a.F + vrow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << a.log_s);
-    const uint32_t c0 = ct << LOG_TC;
-    const int twist_shift = kMaxLog - a.log_s;
-    const uint32_t t = threadIdx.x;
-    uint32_t x[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        uint32_t pos, c;
-        First::elem(t, j, pos, c);
-        const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
-        uint32_t v = FROM_LIMBS ? load_operand(P, a, F, vrow, i, K, q, p, pinv) : F[i];
-        if (INVERSE) {
-            const uint32_t E = ((c0 + c) * bitrev(pos, LOG_R)) << twist_shift;
-            v = mont_mul(v, root_pow(twlo, twhi, E, p, pinv), p, pinv);
-        }
-        x[j] = v;
-    }
-    __syncthreads();   // twiddle table ready
-    run_stages<LOG_R, LOG_TC, INVERSE, 0>(x, Sm, t, tw, p, pinv);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        uint32_t pos, c;
-        Last::elem(t, j, pos, c);
-        const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
-        uint32_t v = x[j];
-        if (!INVERSE) {
-            const uint32_t E = ((c0 + c) * bitrev(pos, LOG_R)) << twist_shift;
-            v = mont_mul(v, root_pow(twlo, twhi, E, p, pinv), p, pinv);
-        }
-        F[i] = v;
-    }
-}
 
 // Fused row pass on C = 2^LOG_C points (T = C/16 threads): forward stages of
 // A then B (A stays in registers while B reuses the shared tile), pointwise
 // product * scale, inverse stages.  The last forward and the first inverse
 // stage share one thread mapping, so the product never leaves registers.
-template <int LOG_C, bool FROM_LIMBS>
-__global__ void __launch_bounds__(kThreads) k_rows_r(NttParams P, RowsArgs a) {
+// The forward twiddle levels are replaced by the inverse ones in the same
+// shared buffer once the forward stages are done.
+template <int LOG_C, bool FROM_LIMBS, int Q>
+__device__ __forceinline__ void rows_body(const NttParams &P, const RowsArgs &a, uint64_t b, uint32_t *Sm,
+                                          uint2 *tw) {
     constexpr int C = 1 << LOG_C;
+    constexpr int T = C / 16;
     constexpr int NS = StagePlan<LOG_C>::n;
     using First = typename ExecStage<LOG_C, 0, false, 0>::S;
-    using Mid = typename ExecStage<LOG_C, 0, false, NS - 1>::S;
     using Out = typename ExecStage<LOG_C, 0, true, NS - 1>::S;
-    __shared__ uint32_t Sm[C + C / 32];
-    __shared__ uint32_t twf[C / 2], twi[C / 2];
-    uint64_t b = blockIdx.x;
-    const int q = (int)(b % kPrimes);
-    b /= kPrimes;
     const uint32_t nseg = 1u << (a.log_k - LOG_C);
     const uint32_t seg = (uint32_t)(b % nseg);
     const uint64_t vrow = b / nseg;
-    const uint64_t brow = a.b_bcast ? (vrow & ((1u << a.coset_bits) - 1u)) : vrow;
-    const PrimeConsts pc = prime_of(P, q);
-    const uint32_t p = pc.p, pinv = pc.pinv;
+    const uint64_t brow = a.b_bcast ? (vrow % (uint32_t)a.M) : vrow;
     const uint64_t K = 1ull << a.log_k;
-    const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + q);
-    const uint32_t *thf = tw_hi_ptr(P.tab, 0, q);
-    const uint32_t *thi = tw_hi_ptr(P.tab, 1, q);
-    for (uint32_t e = threadIdx.x; e < C / 2; e += blockDim.x) {
-        twf[e] = __ldg(thf + (e << (13 - LOG_C)));
-        twi[e] = __ldg(thi + (e << (13 - LOG_C)));
-    }
-    const uint64_t offA = vrow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << LOG_C);
-    const uint64_t offB = brow * 3 * K + (uint64_t)q * K + ((uint64_t)seg << LOG_C);
+    const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + Q);
+    const uint2 *levf = level_ptr(P.tab, 0, Q);
+    const uint2 *levi = level_ptr(P.tab, 1, Q);
+    for (uint32_t e = threadIdx.x; e < C - 1; e += T) tw[e] = __ldg(levf + e);
+    const uint64_t offA = vrow * 3 * K + (uint64_t)Q * K + ((uint64_t)seg << LOG_C);
+    const uint64_t offB = brow * 3 * K + (uint64_t)Q * K + ((uint64_t)seg << LOG_C);
     const uint32_t t = threadIdx.x;
     uint32_t xa[16], xb[16];
 #pragma unroll
@@ -382,28 +285,29 @@ __global__ void __launch_bounds__(kThreads) k_rows_r(NttParams P, RowsArgs a) {
         uint32_t pos, c;
         First::elem(t, j, pos, c);
         if (FROM_LIMBS) {
-            xa[j] = (pos < a.La) ? reduce_limb(a.A[vrow * a.sA + pos], p) : 0u;
-            xb[j] = (!a.square && pos < a.Lb) ? reduce_limb(a.B[brow * a.sB + pos], p) : 0u;
+            xa[j] = (pos < a.La) ? reduce_limb<Q>(__ldg(a.A + vrow * a.sA + pos)) : 0u;
+            xb[j] = (!a.square && pos < a.Lb) ? reduce_limb<Q>(__ldg(a.B + brow * a.sB + pos)) : 0u;
         } else {
             xa[j] = a.FA[offA + pos];
             xb[j] = a.square ? 0u : a.FB[offB + pos];
         }
     }
     __syncthreads();
-    run_stages<LOG_C, 0, false, 0>(xa, Sm, t, twf, p, pinv);
+    run_stages<LOG_C, 0, false, Q, 0>(xa, Sm, t, tw);
     if (!a.square) {
         // the tile is free again: every thread has passed the last stage's loads
         __syncthreads();
-        run_stages<LOG_C, 0, false, 0>(xb, Sm, t, twf, p, pinv);
+        run_stages<LOG_C, 0, false, Q, 0>(xb, Sm, t, tw);
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const uint32_t y = a.square ? xa[j] : xb[j];
-        xa[j] = mont_mul(mont_mul(xa[j], y, p, pinv), scale, p, pinv);
+        xa[j] = norm<Q>(mont<Q>(mont<Q>(xa[j], y), scale));   // x y K^-1
     }
+    __syncthreads();   // forward twiddles and tile no longer read
+    for (uint32_t e = threadIdx.x; e < C - 1; e += T) tw[e] = __ldg(levi + e);
     __syncthreads();
-    run_stages<LOG_C, 0, true, 0>(xa, Sm, t, twi, p, pinv);
-    (void)sizeof(Mid);
+    run_stages<LOG_C, 0, true, Q, 0>(xa, Sm, t, tw);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         uint32_t pos, c;
@@ -412,15 +316,133 @@ __global__ void __launch_bounds__(kThreads) k_rows_r(NttParams P, RowsArgs a) {
     }
 }
 
-__device__ __forceinline__ void garner(const NttParams &P, uint32_t r0, uint32_t r1, uint32_t r2,
-                                       uint32_t (&out)[3]) {
-    const uint32_t p1 = P.pr[1].p, q1 = P.pr[1].pinv;
-    const uint32_t p2 = P.pr[2].p, q2 = P.pr[2].pinv;
-    const uint32_t t1 = mont_mul(sub_mod(r1, r0, p1), P.crt.p0_inv_mod_p1_m, p1, q1);
-    const uint32_t u = mont_mul(sub_mod(r2, r0, p2), P.crt.p0_inv_mod_p2_m, p2, q2);
-    const uint32_t t2 = mont_mul(sub_mod(u, t1, p2), P.crt.p1_inv_mod_p2_m, p2, q2);
-    const unsigned __int128 x =
-        (unsigned __int128)P.crt.p0p1 * t2 + (uint64_t)P.pr[0].p * t1 + r0;
+template <int LOG_C>
+constexpr size_t rows_smem_bytes() {
+    return (size_t)((1 << LOG_C) + (1 << LOG_C) / 32) * 4u + (size_t)((1 << LOG_C) - 1) * 8u;
+}
+
+template <int LOG_C, bool FROM_LIMBS>
+__global__ void __launch_bounds__((1 << LOG_C) / 16) k_rows_r(NttParams P, RowsArgs a) {
+    extern __shared__ uint4 rows_smem[];
+    constexpr int C = 1 << LOG_C;
+    uint32_t *Sm = reinterpret_cast<uint32_t *>(rows_smem);
+    uint2 *tw = reinterpret_cast<uint2 *>(Sm + C + C / 32);
+    uint64_t b;
+    const int q = grid_prime(b);
+    if (q == 0)
+        rows_body<LOG_C, FROM_LIMBS, 0>(P, a, b, Sm, tw);
+    else if (q == 1)
+        rows_body<LOG_C, FROM_LIMBS, 1>(P, a, b, Sm, tw);
+    else
+        rows_body<LOG_C, FROM_LIMBS, 2>(P, a, b, Sm, tw);
+}
+
+// Whole product of K <= 2^8 points per CTA (one prime, one row), radix-2
+// levels in shared memory.
+constexpr int kSmallLog = 8;
+
+template <int Q>
+__device__ __forceinline__ void rows_small_body(const NttParams &P, const RowsArgs &a, uint64_t row,
+                                                uint32_t *SA, uint32_t *SB, uint2 *twf, uint2 *twi) {
+    const int log_k = a.log_k;
+    const uint32_t K = 1u << log_k;
+    const uint64_t brow = a.b_bcast ? 0u : row;
+    const uint32_t scale = __ldg(P.tab.inv2n + log_k * kPrimes + Q);
+    const uint2 *levf = level_ptr(P.tab, 0, Q) + (K / 2 - 1u);   // top level: w_K^e, e < K/2
+    const uint2 *levi = level_ptr(P.tab, 1, Q) + (K / 2 - 1u);
+    for (uint32_t e = threadIdx.x; e < K / 2; e += blockDim.x) {
+        twf[e] = __ldg(levf + e);
+        twi[e] = __ldg(levi + e);
+    }
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
+        SA[i] = (i < a.La) ? reduce_limb<Q>(__ldg(a.A + row * a.sA + i)) : 0u;
+        SB[i] = (!a.square && i < a.Lb) ? reduce_limb<Q>(__ldg(a.B + brow * a.sB + i)) : 0u;
+    }
+    __syncthreads();
+    tile_transform<Q, false>(SA, log_k, 0, twf);
+    if (!a.square) tile_transform<Q, false>(SB, log_k, 0, twf);
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) {
+        const uint32_t x = SA[i];
+        const uint32_t y = a.square ? x : SB[i];
+        SA[i] = norm<Q>(mont<Q>(mont<Q>(x, y), scale));
+    }
+    __syncthreads();
+    tile_transform<Q, true>(SA, log_k, 0, twi);
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) a.FA[row * 3 * K + (uint64_t)Q * K + i] = SA[i];
+}
+
+__global__ void __launch_bounds__(128) k_rows_small(NttParams P, RowsArgs a) {
+    __shared__ uint32_t SA[1 << kSmallLog], SB[1 << kSmallLog];
+    __shared__ uint2 twf[1 << (kSmallLog - 1)], twi[1 << (kSmallLog - 1)];
+    uint64_t row;
+    const int q = grid_prime(row);
+    if (q == 0)
+        rows_small_body<0>(P, a, row, SA, SB, twf, twi);
+    else if (q == 1)
+        rows_small_body<1>(P, a, row, SA, SB, twf, twi);
+    else
+        rows_small_body<2>(P, a, row, SA, SB, twf, twi);
+}
+
+// Coset recombination.  Row r holds z_i[j] = C_i[j] g^(ij) for cosets i < M;
+// C_i[j] = sum_b C_b[j] c_i^b, so C_b[j] = sum_i Vinv[b][i] C_i[j].  The M
+// outputs of position j overwrite the M inputs of position j.
+struct CombineArgs {
+    uint32_t *F;
+    int log_k;
+    uint32_t vinv[kPrimes][kMaxCosets][kMaxCosets];   // Montgomery form, [q][b][i]
+};
+
+template <int M, int Q>
+__device__ __forceinline__ void combine_body(const NttParams &P, const CombineArgs &a, uint64_t row, uint32_t j) {
+    const uint64_t K = 1ull << a.log_k;
+    uint32_t *F0 = a.F + row * M * 3 * K + (uint64_t)Q * K + j;
+    const uint32_t *clo = coset_lo_ptr(P.tab, 1, Q);
+    const uint32_t *chi = coset_hi_ptr(P.tab, 1, Q);
+    uint32_t u[M];
+    u[0] = F0[0];
+#pragma unroll
+    for (int i = 1; i < M; ++i) u[i] = mul_coset<Q>(F0[(uint64_t)i * 3 * K], clo, chi, (uint32_t)i * j);
+#pragma unroll
+    for (int b = 0; b < M; ++b) {
+        uint32_t acc = 0u;
+#pragma unroll
+        for (int i = 0; i < M; ++i) acc = add_n<Q>(acc, norm<Q>(mont<Q>(u[i], a.vinv[Q][b][i])));
+        F0[(uint64_t)b * 3 * K] = acc;
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kThreads) k_combine(NttParams P, CombineArgs a) {
+    uint64_t rest;
+    const int q = grid_prime(rest);
+    const uint32_t jblocks = (1u << a.log_k) / kThreads;
+    const uint64_t row = rest / jblocks;
+    const uint32_t j = (uint32_t)(rest - row * jblocks) * kThreads + threadIdx.x;
+    if (q == 0)
+        combine_body<M, 0>(P, a, row, j);
+    else if (q == 1)
+        combine_body<M, 1>(P, a, row, j);
+    else
+        combine_body<M, 2>(P, a, row, j);
+}
+
+// Garner: residues (r0, r1, r2) -> coefficient < p0 p1 p2 as 3 limbs.
+//   t1 = (r1 - r0) / p0 mod p1,  t2 = ((r2 - r0) / p0 - t1) / p1 mod p2,
+//   x  = r0 + p0 t1 + p0 p1 t2.
+constexpr uint32_t kI01 = cinv(Prime<0>::p, Prime<1>::p);
+constexpr uint32_t kI02 = cinv(Prime<0>::p, Prime<2>::p);
+constexpr uint32_t kI12 = cinv(Prime<1>::p, Prime<2>::p);
+constexpr uint32_t kI01q = shoup_of(kI01, Prime<1>::p);
+constexpr uint32_t kI02q = shoup_of(kI02, Prime<2>::p);
+constexpr uint32_t kI12q = shoup_of(kI12, Prime<2>::p);
+constexpr uint64_t kP0P1 = (uint64_t)Prime<0>::p * Prime<1>::p;
+
+__device__ __forceinline__ void garner(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t (&out)[3]) {
+    const uint32_t t1 = norm<1>(shoup<1>(sub_n<1>(r1, r0), kI01, kI01q));   // r0 < p0 < p1
+    const uint32_t u = norm<2>(shoup<2>(sub_n<2>(r2, r0), kI02, kI02q));
+    const uint32_t t2 = norm<2>(shoup<2>(sub_n<2>(u, t1), kI12, kI12q));    // t1 < p1 < p2
+    const unsigned __int128 x = (unsigned __int128)kP0P1 * t2 + (uint64_t)Prime<0>::p * t1 + r0;
     out[0] = (uint32_t)x;
     out[1] = (uint32_t)(x >> 32);
     out[2] = (uint32_t)(x >> 64);
@@ -432,6 +454,7 @@ constexpr uint32_t kCrtSpan = kThreads * kCrtV;   // 1024 limbs per tile
 struct CrtArgs {
     const uint32_t *F;
     int log_k;
+    int M;
     uint32_t *C;
     uint64_t sC;
     uint32_t Lc;
@@ -439,48 +462,31 @@ struct CrtArgs {
     uint32_t *flags;
 };
 
-// Residue mod p_q of convolution coefficient n.  Without cosets it is read
-// directly.  With two cosets (K = transform length, product length <= 2K) the
-// row holds r0 = C mod (x^K - 1) and beta^i * r1, r1 = C mod (x^K - c1):
-// C_high = (r1 - r0) / (c1 - 1), C_low = r0 - C_high.
-template <bool COSET>
-__device__ __forceinline__ uint32_t coef_residue(const NttParams &P, const uint32_t *F0, uint64_t K, int q,
-                                                 uint64_t n) {
-    if (!COSET) return F0[(uint64_t)q * K + n];
-    const PrimeConsts pc = prime_of(P, q);
-    const uint32_t p = pc.p, pinv = pc.pinv;
-    const uint64_t i = n & (K - 1);
-    const uint32_t r0 = F0[(uint64_t)q * K + i];
-    const uint32_t s1 = F0[3 * K + (uint64_t)q * K + i];
-    const uint32_t r1 =
-        mont_mul(s1, root_pow(beta_lo_ptr(P.tab, 1, q), beta_hi_ptr(P.tab, 1, q), (uint32_t)i, p, pinv), p, pinv);
-    const uint32_t hi = mont_mul(sub_mod(r1, r0, p), sel3(P.coset_cm1_inv, q), p, pinv);
-    return (n >= K) ? hi : sub_mod(r0, hi, p);
-}
-
-template <bool COSET>
-__device__ __forceinline__ void crt_chunk(const NttParams &P, const uint32_t *F0, uint64_t K,
-                                          uint32_t Lc, int64_t base, uint32_t (&S)[kCrtV + 3]) {
+// Coefficient n of a row lives in block b = n / K at F0[(b * 3 + q) * K + n mod K];
+// there are ncoef = L_c - 1 <= M K of them (the top limb only receives carries).
+__device__ __forceinline__ void crt_chunk(const uint32_t *F0, int log_k, uint32_t ncoef, int64_t base,
+                                          uint32_t (&S)[kCrtV + 3]) {
     uint32_t c[kCrtV][3];
-    const uint64_t span = COSET ? 2 * K : K;
-    if (!COSET && base >= 0 && (uint64_t)base + kCrtV <= K && base + kCrtV <= (int64_t)Lc) {
-        // whole chunk inside the row: one 128-bit load per prime (K and base are multiples of 4)
-        const uint4 r0 = *reinterpret_cast<const uint4 *>(F0 + base);
-        const uint4 r1 = *reinterpret_cast<const uint4 *>(F0 + K + base);
-        const uint4 r2 = *reinterpret_cast<const uint4 *>(F0 + 2 * K + base);
-        garner(P, r0.x, r1.x, r2.x, c[0]);
-        garner(P, r0.y, r1.y, r2.y, c[1]);
-        garner(P, r0.z, r1.z, r2.z, c[2]);
-        garner(P, r0.w, r1.w, r2.w, c[3]);
+    const uint64_t K = 1ull << log_k;
+    if (base >= 0 && base + kCrtV <= (int64_t)ncoef && K >= (uint64_t)kCrtV) {
+        // the chunk lies in one block: one 128-bit load per prime (K and base are multiples of 4)
+        const uint64_t off = (((uint64_t)base >> log_k) * 3) * K + ((uint64_t)base & (K - 1));
+        const uint4 r0 = *reinterpret_cast<const uint4 *>(F0 + off);
+        const uint4 r1 = *reinterpret_cast<const uint4 *>(F0 + off + K);
+        const uint4 r2 = *reinterpret_cast<const uint4 *>(F0 + off + 2 * K);
+        garner(r0.x, r1.x, r2.x, c[0]);
+        garner(r0.y, r1.y, r2.y, c[1]);
+        garner(r0.z, r1.z, r2.z, c[2]);
+        garner(r0.w, r1.w, r2.w, c[3]);
         chunk_sum3<kCrtV>(c, S);
         return;
     }
 #pragma unroll
     for (int v = 0; v < kCrtV; ++v) {
         const int64_t i = base + v;
-        if (i >= 0 && (uint64_t)i < span && i < (int64_t)Lc) {
-            garner(P, coef_residue<COSET>(P, F0, K, 0, i), coef_residue<COSET>(P, F0, K, 1, i),
-                   coef_residue<COSET>(P, F0, K, 2, i), c[v]);
+        if (i >= 0 && i < (int64_t)ncoef) {
+            const uint64_t off = (((uint64_t)i >> log_k) * 3) * K + ((uint64_t)i & (K - 1));
+            garner(F0[off], F0[off + K], F0[off + 2 * K], c[v]);
         } else {
             c[v][0] = c[v][1] = c[v][2] = 0u;
         }
@@ -488,24 +494,23 @@ __device__ __forceinline__ void crt_chunk(const NttParams &P, const uint32_t *F0
     chunk_sum3<kCrtV>(c, S);
 }
 
-template <bool COSET>
-__global__ void __launch_bounds__(kThreads) k_crt(NttParams P, CrtArgs a) {
+__global__ void __launch_bounds__(kThreads) k_crt(CrtArgs a) {
     __shared__ uint32_t sg[kThreads / 32], sp[kThreads / 32], spre[kThreads / 32];
     const uint32_t tile = blockIdx.x;
     const uint64_t row = tile / a.tiles;
     const uint32_t t = tile - (uint32_t)row * a.tiles;
     const uint64_t K = 1ull << a.log_k;
-    const uint32_t *F0 = a.F + row * (COSET ? 6 : 3) * K;
+    const uint32_t *F0 = a.F + row * (uint64_t)a.M * 3 * K;
     const int64_t base = (int64_t)t * kCrtSpan + threadIdx.x * kCrtV;
     uint32_t S[kCrtV + 3];
-    crt_chunk<COSET>(P, F0, K, a.Lc, base, S);
+    crt_chunk(F0, a.log_k, a.Lc - 1u, base, S);
     uint32_t H[3];
     H[0] = __shfl_up_sync(0xffffffffu, S[kCrtV], 1);
     H[1] = __shfl_up_sync(0xffffffffu, S[kCrtV + 1], 1);
     H[2] = __shfl_up_sync(0xffffffffu, S[kCrtV + 2], 1);
     if (lane_id() == 0) {
         uint32_t Sp[kCrtV + 3];
-        crt_chunk<COSET>(P, F0, K, a.Lc, base - kCrtV, Sp);
+        crt_chunk(F0, a.log_k, a.Lc - 1u, base - kCrtV, Sp);
         H[0] = Sp[kCrtV];
         H[1] = Sp[kCrtV + 1];
         H[2] = Sp[kCrtV + 2];
@@ -540,48 +545,21 @@ static int ceil_log2(uint64_t x) {
     return k;
 }
 
-static int transform_log(uint32_t La, uint32_t Lb) {
+struct Shape {
+    int log_k;   // K = 2^log_k points per coset
+    int M;       // cosets
+};
+
+// Smallest shape with M * K >= L_a + L_b - 1: one power-of-two transform up to
+// 2^25 points, above that M cosets of 2^25 points.
+static Shape shape_for(uint32_t La, uint32_t Lb) {
     const uint64_t need = (uint64_t)La + Lb - 1u;
-    int k = ceil_log2(need < 2 ? 2 : need);
-    return k < 1 ? 1 : k;
-}
-
-template <class Kern>
-static void set_smem(Kern kern, size_t bytes) {
-    if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
-static void launch_cols(bool from_limbs, bool inverse, const NttParams &P, const ColsArgs &a,
-                        uint64_t vrows, cudaStream_t st) {
-    const uint64_t ctiles = 1ull << (a.log_s - a.log_r - a.log_tc);
-    const uint64_t nseg = 1ull << (a.log_k - a.log_s);
-    const uint64_t blocks = vrows * kPrimes * nseg * ctiles;
-    const size_t smem = ((size_t(1) << (a.log_r + a.log_tc)) + (size_t(1) << (a.log_r - 1))) * 4;
-    // algorithmic bytes: 12 B per coefficient (3 primes x 4 B) read and written;
-    // the first pass reads each limb once instead
-    const double K = (double)(1ull << a.log_k);
-    const double bytes = from_limbs ? (4.0 * a.Lx * (double)(vrows >> a.coset_bits) + 12.0 * K * (double)vrows)
-                                    : 24.0 * K * (double)vrows;
-    KernelTimed kt(from_limbs ? "ntt_cols_fwd_first" : (inverse ? "ntt_cols_inv" : "ntt_cols_fwd"), bytes);
-    if (from_limbs) {
-        set_smem(k_cols<true, false>, smem);
-        k_cols<true, false><<<(unsigned)blocks, kThreads, smem, st>>>(P, a);
-    } else if (!inverse) {
-        set_smem(k_cols<false, false>, smem);
-        k_cols<false, false><<<(unsigned)blocks, kThreads, smem, st>>>(P, a);
-    } else {
-        set_smem(k_cols<false, true>, smem);
-        k_cols<false, true><<<(unsigned)blocks, kThreads, smem, st>>>(P, a);
+    if (need <= (1ull << kMaxLog)) {
+        const int k = ceil_log2(need < 2 ? 2 : need);
+        return {k < 1 ? 1 : k, 1};
     }
-    count_launch();
-}
-
-static bool use_radix2() {
-    static const bool v = [] {
-        const char *e = getenv("GPUPI_NTT_RADIX2");
-        return e && e[0] == '1';
-    }();
-    return v;
+    const uint64_t K = 1ull << kMaxLog;
+    return {kMaxLog, (int)((need + K - 1) / K)};
 }
 
 template <bool FL, bool INV>
@@ -599,48 +577,110 @@ static void cols_r_dispatch(int log_r, unsigned blocks, const NttParams &P, cons
     }
 }
 
-static void launch_cols_r(bool from_limbs, bool inverse, const NttParams &P, const ColsArgs &a, uint64_t vrows,
-                          cudaStream_t st) {
-    const uint64_t ctiles = 1ull << (a.log_s - a.log_r - (12 - a.log_r));
+static void launch_cols_r(bool from_limbs, bool inverse, int log_r, const NttParams &P, const ColsArgs &a,
+                          uint64_t vrows, cudaStream_t st) {
+    const uint64_t ctiles = 1ull << (a.log_s - 12);
     const uint64_t nseg = 1ull << (a.log_k - a.log_s);
     const unsigned blocks = (unsigned)(vrows * kPrimes * nseg * ctiles);
+    // algorithmic bytes: 12 B per point (3 primes x 4 B) read and written;
+    // the first pass reads the limbs instead (once per coset)
     const double K = (double)(1ull << a.log_k);
-    const double bytes = from_limbs ? (4.0 * a.Lx * (double)(vrows >> a.coset_bits) + 12.0 * K * (double)vrows)
+    const double bytes = from_limbs ? (4.0 * a.Lx * (double)vrows / a.M + 12.0 * K * (double)vrows)
                                     : 24.0 * K * (double)vrows;
     KernelTimed kt(from_limbs ? "ntt_cols_fwd_first" : (inverse ? "ntt_cols_inv" : "ntt_cols_fwd"), bytes);
     if (from_limbs)
-        cols_r_dispatch<true, false>(a.log_r, blocks, P, a, st);
+        cols_r_dispatch<true, false>(log_r, blocks, P, a, st);
     else if (!inverse)
-        cols_r_dispatch<false, false>(a.log_r, blocks, P, a, st);
+        cols_r_dispatch<false, false>(log_r, blocks, P, a, st);
     else
-        cols_r_dispatch<false, true>(a.log_r, blocks, P, a, st);
+        cols_r_dispatch<false, true>(log_r, blocks, P, a, st);
     count_launch();
+}
+
+template <int LOG_C, bool FL>
+static void rows_launch(unsigned blocks, const NttParams &P, const RowsArgs &r, cudaStream_t st) {
+    constexpr size_t smem = rows_smem_bytes<LOG_C>();
+    static bool attr = false;
+    if (!attr) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_rows_r<LOG_C, FL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_rows_r<LOG_C, FL><<<blocks, (1 << LOG_C) / 16, smem, st>>>(P, r);
 }
 
 template <bool FL>
 static void rows_r_dispatch(int log_c, unsigned blocks, const NttParams &P, const RowsArgs &r, cudaStream_t st) {
     switch (log_c) {
-        case 9: k_rows_r<9, FL><<<blocks, 32, 0, st>>>(P, r); break;
-        case 10: k_rows_r<10, FL><<<blocks, 64, 0, st>>>(P, r); break;
-        case 11: k_rows_r<11, FL><<<blocks, 128, 0, st>>>(P, r); break;
-        default: k_rows_r<12, FL><<<blocks, 256, 0, st>>>(P, r); break;
+        case 9: rows_launch<9, FL>(blocks, P, r, st); break;
+        case 10: rows_launch<10, FL>(blocks, P, r, st); break;
+        case 11: rows_launch<11, FL>(blocks, P, r, st); break;
+        default: rows_launch<12, FL>(blocks, P, r, st); break;
     }
 }
 
-static int tc_for(int log_r, int log_cols) {
-    int log_tc = 12 - log_r;
-    if (log_tc < 4) log_tc = 4;
-    if (log_tc > log_cols) log_tc = log_cols;
-    return log_tc;
+// Inverse of the Vandermonde matrix V[i][b] = c_i^b (c_i = g^(i 2^log_k)) mod
+// p_q, Montgomery form, out[q][b][i].
+static void coset_matrix(int M, int log_k, uint32_t (&out)[kPrimes][kMaxCosets][kMaxCosets]) {
+    for (int q = 0; q < kPrimes; ++q) {
+        const uint32_t p = kP[q];
+        uint32_t V[kMaxCosets][2 * kMaxCosets] = {};
+        for (int i = 0; i < M; ++i) {
+            const uint32_t c = h_pow(kGen[q], (uint64_t)i << log_k, p);
+            uint32_t x = 1u;
+            for (int b = 0; b < M; ++b) {
+                V[i][b] = x;
+                x = h_mul(x, c, p);
+            }
+            V[i][M + i] = 1u;
+        }
+        for (int col = 0; col < M; ++col) {   // Gauss-Jordan; the nodes are distinct
+            int piv = col;
+            while (V[piv][col] == 0u) ++piv;
+            if (piv != col)
+                for (int k = 0; k < 2 * M; ++k) {
+                    const uint32_t tmp = V[piv][k];
+                    V[piv][k] = V[col][k];
+                    V[col][k] = tmp;
+                }
+            const uint32_t inv = h_inv(V[col][col], p);
+            for (int k = 0; k < 2 * M; ++k) V[col][k] = h_mul(V[col][k], inv, p);
+            for (int r = 0; r < M; ++r) {
+                if (r == col || V[r][col] == 0u) continue;
+                const uint32_t f = V[r][col];
+                for (int k = 0; k < 2 * M; ++k)
+                    V[r][k] = (uint32_t)((V[r][k] + (uint64_t)(p - h_mul(f, V[col][k], p))) % p);
+            }
+        }
+        for (int b = 0; b < kMaxCosets; ++b)
+            for (int i = 0; i < kMaxCosets; ++i)
+                out[q][b][i] = (b < M && i < M) ? h_mont(V[b][M + i], p) : 0u;
+    }
+}
+
+static void launch_combine(int M, const NttParams &P, const CombineArgs &c, uint32_t N, cudaStream_t st) {
+    const uint64_t K = 1ull << c.log_k;
+    const unsigned blocks = (unsigned)((uint64_t)N * kPrimes * (K / kThreads));
+    KernelTimed kt("ntt_coset_combine", 24.0 * (double)K * M * N);
+    switch (M) {
+        case 2: k_combine<2><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 3: k_combine<3><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 4: k_combine<4><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 5: k_combine<5><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 6: k_combine<6><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 7: k_combine<7><<<blocks, kThreads, 0, st>>>(P, c); break;
+        default: k_combine<8><<<blocks, kThreads, 0, st>>>(P, c); break;
+    }
+    count_launch();
 }
 
 size_t workspace_bytes(uint32_t N, uint32_t La, uint32_t Lb) {
     if (N == 0u || La == 0u || Lb == 0u) return 0;
-    const int log_k = transform_log(La, Lb);
-    const uint64_t K = 1ull << log_k;
+    const Shape s = shape_for(La, Lb);
+    const uint64_t K = 1ull << s.log_k;
     const uint64_t Lc = (uint64_t)La + Lb;
     const uint64_t tiles = (Lc + kCrtSpan - 1) / kCrtSpan;
-    return (size_t)(2ull * N * 3 * K * 4 + N * tiles * 4 + 256);
+    return (size_t)(2ull * N * s.M * 3 * K * 4 + N * tiles * 4 + 256);
 }
 
 static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t *ws,
@@ -652,16 +692,14 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         cudaMemset2DAsync(C, sC * 4, 0, (size_t)Lc * 4, N, st);
         return;
     }
-    const int log_total = transform_log(La, Lb);
-    if (log_total > kMaxLog + 1) {
+    const Shape s = shape_for(La, Lb);
+    if (s.M > kMaxCosets) {
         fprintf(stderr, "gpupi_b200: product of %u limbs exceeds the 2^28-point limit\n", Lc);
         return;
     }
-    // Above 2^27 points the product is split into two cosets of 2^27 points.
-    const int cb = (log_total > kMaxLog) ? 1 : 0;
-    const int log_k = log_total - cb;
+    const int log_k = s.log_k, M = s.M;
     const uint64_t K = 1ull << log_k;
-    const uint64_t VR = (uint64_t)N << cb;   // virtual rows (row, coset)
+    const uint64_t VR = (uint64_t)N * M;   // virtual rows (row, coset)
     const bool square = (A == B && La == Lb && sA == sB);
     const bool bcast = (!square && sB == 0u && N > 1u);
     uint32_t *FA = ws;
@@ -670,23 +708,19 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
     uint32_t *flags = ws + 2ull * VR * 3 * K;
 
     if (log_k <= 12) {
-        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_k, bcast ? 1 : 0, square ? 1 : 0, 0};
+        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, 1, bcast ? 1 : 0, square ? 1 : 0};
         KernelTimed kt("ntt_local", 4.0 * N * ((double)La + (square ? 0 : Lb)) + 12.0 * K * N);
-        if (log_k >= 9 && !use_radix2()) {
+        if (log_k >= 9)
             rows_r_dispatch<true>(log_k, (unsigned)(N * kPrimes), P, r, st);
-        } else {
-            const size_t smem = (size_t)3 * K * 4;
-            set_smem(k_rows<true>, smem);
-            k_rows<true><<<(unsigned)(N * kPrimes), kThreads, smem, st>>>(P, r);
-        }
+        else
+            k_rows_small<<<(unsigned)(N * kPrimes), 128, 0, st>>>(P, r);
         count_launch();
     } else {
         const int log_c = 12;
         const int rest = log_k - log_c;
-        const bool r2 = use_radix2();
         int passes[2];
         int npass;
-        if (rest <= (r2 ? 10 : 9)) {
+        if (rest <= 9) {
             passes[0] = rest;
             npass = 1;
         } else {
@@ -700,53 +734,40 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
             const uint64_t sX = op == 0 ? sA : sB;
             const uint32_t Lx = op == 0 ? La : Lb;
             uint32_t *F = op == 0 ? FA : FB;
-            const uint64_t vrows = (op == 1 && bcast) ? (1ull << cb) : VR;
+            const uint64_t vrows = (op == 1 && bcast) ? (uint64_t)M : VR;
+            const uint32_t nb = (uint32_t)((Lx + K - 1) / K);
             int log_s = log_k;
             for (int ps = 0; ps < npass; ++ps) {
-                ColsArgs a{X, sX, Lx, F, log_k, log_s, passes[ps], 0, cb};
-                if (r2) {
-                    a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
-                    launch_cols(ps == 0, false, P, a, vrows, st);
-                } else {
-                    a.log_tc = 12 - passes[ps];
-                    launch_cols_r(ps == 0, false, P, a, vrows, st);
-                }
+                ColsArgs a{X, sX, Lx, nb, F, log_k, log_s, M};
+                launch_cols_r(ps == 0, false, passes[ps], P, a, vrows, st);
                 log_s -= passes[ps];
             }
         }
-        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, log_c, bcast ? 1 : 0, square ? 1 : 0, cb};
+        RowsArgs r{A, sA, La, B, sB, Lb, FA, FB, log_k, M, bcast ? 1 : 0, square ? 1 : 0};
         const uint64_t blocks = VR * kPrimes * (K >> log_c);
         {
             KernelTimed kt("ntt_rows_fused", 12.0 * (double)K * ((square ? 2.0 : 3.0) * (double)VR));
-            if (r2) {
-                const size_t smem = (size_t)3 * (1u << log_c) * 4;
-                set_smem(k_rows<false>, smem);
-                k_rows<false><<<(unsigned)blocks, kThreads, smem, st>>>(P, r);
-            } else {
-                rows_r_dispatch<false>(log_c, (unsigned)blocks, P, r, st);
-            }
+            rows_r_dispatch<false>(log_c, (unsigned)blocks, P, r, st);
             count_launch();
         }
         // inverse column passes, innermost first
         int log_s = log_c;
         for (int ps = npass - 1; ps >= 0; --ps) {
             log_s += passes[ps];
-            ColsArgs a{nullptr, 0, 0, FA, log_k, log_s, passes[ps], 0, 0};
-            if (r2) {
-                a.log_tc = tc_for(passes[ps], log_s - passes[ps]);
-                launch_cols(false, true, P, a, VR, st);
-            } else {
-                a.log_tc = 12 - passes[ps];
-                launch_cols_r(false, true, P, a, VR, st);
-            }
+            ColsArgs a{nullptr, 0, 0, 0, FA, log_k, log_s, M};
+            launch_cols_r(false, true, passes[ps], P, a, VR, st);
+        }
+        if (M > 1) {
+            CombineArgs c{};
+            c.F = FA;
+            c.log_k = log_k;
+            coset_matrix(M, log_k, c.vinv);
+            launch_combine(M, P, c, N, st);
         }
     }
-    CrtArgs c{FA, log_k, C, sC, Lc, (uint32_t)tiles, flags};
+    CrtArgs c{FA, log_k, M, C, sC, Lc, (uint32_t)tiles, flags};
     KernelTimed kt("ntt_crt_carry", 12.0 * (double)Lc * N + 4.0 * (double)Lc * N);
-    if (cb)
-        k_crt<true><<<(unsigned)(N * tiles), kThreads, 0, st>>>(P, c);
-    else
-        k_crt<false><<<(unsigned)(N * tiles), kThreads, 0, st>>>(P, c);
+    k_crt<<<(unsigned)(N * tiles), kThreads, 0, st>>>(c);
     count_launch();
     if (tiles > 1) launch_carry_fixup(false, C, sC, N, Lc, (uint32_t)tiles, kCrtSpan, flags, st);
 }
@@ -757,34 +778,47 @@ void build_tables(std::vector<uint32_t> &lv1, std::vector<uint32_t> &lv2, std::v
     inv2n.assign(33u * 3u, 0u);
     for (int q = 0; q < kPrimes; ++q) {
         const uint32_t p = kP[q];
-        const uint32_t w = h_pow(kGen[q], (p - 1u) >> kMaxLog, p);
-        const uint32_t beta = kGen[q];
+        const uint32_t g = kGen[q];
+        const uint32_t w = h_pow(g, (p - 1u) >> kMaxLog, p);   // primitive 2^25-th root
         for (int dir = 0; dir < 2; ++dir) {
             const uint32_t base = dir ? h_inv(w, p) : w;
-            const uint32_t bb = dir ? h_inv(beta, p) : beta;
             uint32_t x = 1u;
             for (uint32_t e = 0; e < kLoSize; ++e) {
-                lv1[(size_t)(dir * kPrimes + q) * kLoSize + e] = h_mont(x, p);
+                const size_t o = ((size_t)(dir * kPrimes + q) * kLoSize + e) * 2u;
+                lv1[o] = x;
+                lv1[o + 1] = shoup_of(x, p);
                 x = h_mul(x, base, p);
             }
             const uint32_t step = h_pow(base, kLoSize, p);
             x = 1u;
             for (uint32_t e = 0; e < kHiSize; ++e) {
-                lv2[(size_t)(dir * kPrimes + q) * kHiSize + e] = h_mont(x, p);
+                const size_t o = kRootLoWords + ((size_t)(dir * kPrimes + q) * kHiSize + e) * 2u;
+                lv1[o] = x;
+                lv1[o + 1] = shoup_of(x, p);
                 x = h_mul(x, step, p);
             }
-            const size_t blo = 2u * kPrimes * kHiSize;
-            const size_t bhi = blo + 2u * kPrimes * kLoSize;
-            x = 1u;
-            for (uint32_t e = 0; e < kLoSize; ++e) {
-                lv2[blo + (size_t)(dir * kPrimes + q) * kLoSize + e] = h_mont(x, p);
-                x = h_mul(x, bb, p);
+            for (int lh = 0; lh < kLevelLogMax; ++lh) {
+                const uint32_t root = h_pow(base, 1ull << (kMaxLog - 1 - lh), p);   // w_(2h), h = 2^lh
+                x = 1u;
+                for (uint32_t m = 0; m < (1u << lh); ++m) {
+                    const size_t o =
+                        kLevelOffset + ((size_t)(dir * kPrimes + q) * kLevelSize + (1u << lh) - 1u + m) * 2u;
+                    lv1[o] = x;
+                    lv1[o + 1] = shoup_of(x, p);
+                    x = h_mul(x, root, p);
+                }
             }
-            const uint32_t bstep = h_pow(bb, kLoSize, p);
+            const uint32_t gb = dir ? h_inv(g, p) : g;
             x = 1u;
-            for (uint32_t e = 0; e < kHiSize; ++e) {
-                lv2[bhi + (size_t)(dir * kPrimes + q) * kHiSize + e] = h_mont(x, p);
-                x = h_mul(x, bstep, p);
+            for (uint32_t e = 0; e < kCosetSize; ++e) {
+                lv2[(size_t)(dir * kPrimes + q) * kCosetSize + e] = h_mont(x, p);
+                x = h_mul(x, gb, p);
+            }
+            const uint32_t gstep = h_pow(gb, kCosetSize, p);
+            x = 1u;
+            for (uint32_t e = 0; e < kCosetSize; ++e) {
+                lv2[kCosetWords + (size_t)(dir * kPrimes + q) * kCosetSize + e] = h_mont(x, p);
+                x = h_mul(x, gstep, p);
             }
         }
         const uint32_t r2 = h_mont(h_mont(1u, p), p);   // R^2 mod p

@@ -1,21 +1,22 @@
 // Three-prime number-theoretic transform building blocks (sm_100a).
 //
-// An exact product of 32-bit-limb integers is computed as a cyclic
-// convolution modulo three primes p0 < p1 < p2 (all just below 2^32, product
-// ~2^95.1) and recombined by Garner's CRT.  A convolution coefficient is at
-// most min(L_a, L_b) * (2^32-1)^2 < 2^92 for products up to 2^29 limbs, so
-// the CRT value is the exact coefficient.
+// An exact product of 32-bit-limb integers is a cyclic convolution computed
+// modulo three primes below 2^31 and recombined by Garner's CRT:
 //
-//   p0 = 3 * 2^30 + 1   (2-adicity 30)
-//   p1 = 13 * 2^28 + 1  (2-adicity 28)
-//   p2 = 29 * 2^27 + 1  (2-adicity 27)
+//   p0 = 27 * 2^26 + 1 = 1811939329   (2-adicity 26, generator 13)
+//   p1 = 15 * 2^27 + 1 = 2013265921   (2-adicity 27, generator 31)
+//   p2 = 63 * 2^25 + 1 = 2113929217   (2-adicity 25, generator 5)
 //
-// Direct transforms are limited to 2^27 points (p2's 2-adicity); products of
-// length up to 2^28 are split into the residues mod x^K - 1 and mod
-// x^K - beta^K (two cosets of 2^27 points each).
+// p0 p1 p2 > 2^92.6 and a convolution coefficient is at most
+// min(L_a, L_b) * (2^32 - 1)^2, so every product with min(L_a, L_b) < 2^28
+// is recovered exactly.  Transforms have at most 2^25 points (p2's
+// 2-adicity); longer products are split into cosets (mul_ntt.cu).
 //
-// Arithmetic is Montgomery with R = 2^32 on 32-bit words.  Data stays in plain
-// form; twiddles are stored in Montgomery form, so mont(x, w_M) = x*w.
+// Residues are kept in [0, p).  Since 2p < 2^32 a sum or difference needs
+// one unsigned min to reduce (x - p wraps above x exactly when x < p), and a
+// product by a table constant w uses Shoup's method with w' = floor(w 2^32/p):
+// q = hi(x w'), r = x w - q p lies in [0, 2p) for every 32-bit x.  Products
+// of two variables use Montgomery reduction with R = 2^32.
 #pragma once
 
 #include "common.cuh"
@@ -24,88 +25,171 @@ namespace gpupi {
 namespace ntt {
 
 constexpr int kPrimes = 3;
-constexpr int kMaxLog = 27;          // largest direct transform
-constexpr int kLoBits = 14;          // two-level twiddle split: 2^27 = 2^14 * 2^13
+constexpr int kMaxLog = 25;          // largest transform: 2^25 points
+constexpr int kLoBits = 13;          // root tables: w^e = LO[e mod 2^13] * HI[e >> 13]
 constexpr uint32_t kLoSize = 1u << kLoBits;
-constexpr uint32_t kHiSize = 1u << (kMaxLog - kLoBits);   // 8192
+constexpr uint32_t kHiSize = 1u << (kMaxLog - kLoBits);   // 4096
+constexpr int kCosetLoBits = 14;     // coset tables: g^e for e < 2^28
+constexpr uint32_t kCosetSize = 1u << kCosetLoBits;
+constexpr int kMaxCosets = 8;
 
-struct PrimeConsts {
-    uint32_t p;
-    uint32_t pinv;   // p^-1 mod 2^32
+constexpr uint32_t inv_2_32(uint32_t p) {
+    uint32_t x = p;   // Newton iteration for p^-1 mod 2^32
+    for (int i = 0; i < 5; ++i) x *= 2u - p * x;
+    return x;
+}
+constexpr uint32_t cmul(uint32_t a, uint32_t b, uint32_t p) { return (uint32_t)((uint64_t)a * b % p); }
+constexpr uint32_t cpow(uint32_t a, uint64_t e, uint32_t p) {
+    uint32_t r = 1u;
+    while (e) {
+        if (e & 1u) r = cmul(r, a, p);
+        a = cmul(a, a, p);
+        e >>= 1;
+    }
+    return r;
+}
+constexpr uint32_t cinv(uint32_t a, uint32_t p) { return cpow(a % p, p - 2u, p); }
+constexpr uint32_t shoup_of(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
+
+template <int Q>
+struct Prime;
+template <>
+struct Prime<0> {
+    static constexpr uint32_t p = 1811939329u, g = 13u;
 };
-
-// Table layout inside NTTPrecomputedTables (raw u32 views of the uint3 buffers):
-//   lv1: [dir][prime][kLoSize]  TW_LO[e]   = w^e            (w = primitive 2^27-th root; dir 1 = w^-1)
-//   lv2: [dir][prime][kHiSize]  TW_HI[e]   = w^(e * 2^14)   (= 8192-th roots)
-//        then [dir][prime][kLoSize] BETA_LO[e] = beta^e, [dir][prime][kHiSize] BETA_HI[e] = beta^(e*2^14)
-//   inv2n: [k][prime]           K^-1 * R^2 mod p  (K = 2^k), folds the 1/K of the
-//                                inverse and the R^-1 of the pointwise product
-//   Everything in Montgomery form.
-struct Tables {
-    const uint32_t *tw_lo;     // lv1
-    const uint32_t *tw_hi;     // lv2
-    const uint32_t *beta_lo;   // lv2 + 2*3*kHiSize
-    const uint32_t *beta_hi;   // beta_lo + 2*3*kLoSize
-    const uint32_t *inv2n;     // 33*3
+template <>
+struct Prime<1> {
+    static constexpr uint32_t p = 2013265921u, g = 31u;
 };
+template <>
+struct Prime<2> {
+    static constexpr uint32_t p = 2113929217u, g = 5u;
+};
+template <int Q>
+struct PrimeC {
+    static constexpr uint32_t p = Prime<Q>::p;
+    static constexpr uint32_t pinv = inv_2_32(p);
+    static constexpr uint32_t r1 = (uint32_t)((1ull << 32) % p);   // R mod p: Montgomery form of 1
+};
+static_assert(PrimeC<0>::p * PrimeC<0>::pinv == 1u, "p0 inverse");
+static_assert(PrimeC<1>::p * PrimeC<1>::pinv == 1u, "p1 inverse");
+static_assert(PrimeC<2>::p * PrimeC<2>::pinv == 1u, "p2 inverse");
 
-__device__ __forceinline__ const uint32_t *tw_lo_ptr(const Tables &t, int dir, int q) {
-    return t.tw_lo + ((size_t)dir * kPrimes + q) * kLoSize;
+// x in [0, 2p) -> [0, p)
+template <int Q>
+__device__ __forceinline__ uint32_t norm(uint32_t x) {
+    return min(x, x - Prime<Q>::p);
 }
-__device__ __forceinline__ const uint32_t *tw_hi_ptr(const Tables &t, int dir, int q) {
-    return t.tw_hi + ((size_t)dir * kPrimes + q) * kHiSize;
+template <int Q>
+__device__ __forceinline__ uint32_t add_n(uint32_t a, uint32_t b) {
+    return norm<Q>(a + b);
 }
-__device__ __forceinline__ const uint32_t *beta_lo_ptr(const Tables &t, int dir, int q) {
-    return t.beta_lo + ((size_t)dir * kPrimes + q) * kLoSize;
+template <int Q>
+__device__ __forceinline__ uint32_t sub_n(uint32_t a, uint32_t b) {
+    return norm<Q>(a - b + Prime<Q>::p);
 }
-__device__ __forceinline__ const uint32_t *beta_hi_ptr(const Tables &t, int dir, int q) {
-    return t.beta_hi + ((size_t)dir * kPrimes + q) * kHiSize;
+// x < 2^32 (< 3p) -> [0, p)
+template <int Q>
+__device__ __forceinline__ uint32_t reduce_limb(uint32_t x) {
+    return norm<Q>(min(x, x - Prime<Q>::p));
 }
-
-__device__ __forceinline__ uint32_t mont_mul(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
-    // a*b < p*2^32 required (a < 2^32, b < p).  Result in [0, p).
+// x * w mod p in [0, 2p), w < p with wq = floor(w 2^32 / p), any 32-bit x
+template <int Q>
+__device__ __forceinline__ uint32_t shoup(uint32_t x, uint32_t w, uint32_t wq) {
+    const uint32_t q = __umulhi(x, wq);
+    return x * w - q * Prime<Q>::p;
+}
+// a * b / 2^32 mod p in (0, 2p); requires a * b < 2^32 * p
+template <int Q>
+__device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b) {
     const uint64_t t = (uint64_t)a * b;
-    const uint32_t tlo = (uint32_t)t;
-    const uint32_t thi = (uint32_t)(t >> 32);
-    const uint32_t m = tlo * pinv;
-    const uint32_t mh = __umulhi(m, p);
-    const uint32_t r = thi - mh;
-    return (thi < mh) ? r + p : r;
+    const uint32_t m = (uint32_t)t * PrimeC<Q>::pinv;
+    return (uint32_t)(t >> 32) - __umulhi(m, Prime<Q>::p) + Prime<Q>::p;
 }
 
-__device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b, uint32_t p) {
-    const uint32_t s = a + b;
-    const uint32_t t = s - p;
-    return (s < a || s >= p) ? t : s;
+// Table layout inside NTTPrecomputedTables (raw u32 views of the uint3 buffers).
+//   lv1: ROOT_LO[dir][q][2^13]  uint2 {w^e, shoup}        w = primitive 2^25-th root,
+//        ROOT_HI[dir][q][2^12]  uint2 {w^(e 2^13), shoup}  dir 1 holds w^-1
+//        LEVEL[dir][q][4095]    uint2 {w_(2h)^m, shoup} at (h - 1) + m for
+//                               h = 2^lh, m < h, lh < 12: the twiddles of
+//                               radix-2 level lh, contiguous per level
+//   lv2: COSET_LO[dir][q][2^14] g^e, COSET_HI[dir][q][2^14] g^(e 2^14), Montgomery
+//        form, dir 1 holds g^-1 (coset twists beta_i^j = g^(i j), i j < 2^28)
+//   inv2n: [k][q]  2^-k * R^2 mod p (scale of the pointwise product)
+constexpr int kLevelLogMax = 12;
+constexpr uint32_t kLevelSize = (1u << kLevelLogMax) - 1u;        // 4095
+constexpr size_t kRootLoWords = 2u * kPrimes * kLoSize * 2u;     // 98304
+constexpr size_t kRootHiWords = 2u * kPrimes * kHiSize * 2u;     // 49152
+constexpr size_t kLevelOffset = kRootLoWords + kRootHiWords;     // 147456
+constexpr size_t kLevelWords = 2u * kPrimes * kLevelSize * 2u;   // 49140
+constexpr size_t kCosetWords = 2u * kPrimes * kCosetSize;        // per level: 98304
+static_assert(kLevelOffset + kLevelWords <= 65536u * 3u, "lv1 capacity");
+static_assert(2u * kCosetWords <= 65536u * 3u, "lv2 capacity");
+
+struct Tables {
+    const uint2 *root_lo;       // [dir][q][kLoSize]
+    const uint2 *root_hi;       // [dir][q][kHiSize]
+    const uint2 *level;         // [dir][q][kLevelSize]
+    const uint32_t *coset_lo;   // [dir][q][kCosetSize]
+    const uint32_t *coset_hi;   // [dir][q][kCosetSize]
+    const uint32_t *inv2n;      // [33][q]
+};
+
+__device__ __forceinline__ const uint2 *root_lo_ptr(const Tables &t, int dir, int q) {
+    return t.root_lo + ((size_t)dir * kPrimes + q) * kLoSize;
+}
+__device__ __forceinline__ const uint2 *root_hi_ptr(const Tables &t, int dir, int q) {
+    return t.root_hi + ((size_t)dir * kPrimes + q) * kHiSize;
+}
+__device__ __forceinline__ const uint2 *level_ptr(const Tables &t, int dir, int q) {
+    return t.level + ((size_t)dir * kPrimes + q) * kLevelSize;
+}
+__device__ __forceinline__ const uint32_t *coset_lo_ptr(const Tables &t, int dir, int q) {
+    return t.coset_lo + ((size_t)dir * kPrimes + q) * kCosetSize;
+}
+__device__ __forceinline__ const uint32_t *coset_hi_ptr(const Tables &t, int dir, int q) {
+    return t.coset_hi + ((size_t)dir * kPrimes + q) * kCosetSize;
 }
 
-__device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t p) {
-    const uint32_t d = a - b;
-    return (a < b) ? d + p : d;
+// x * w^E for E < 2^25 (w the root table's root), result in [0, p)
+template <int Q>
+__device__ __forceinline__ uint32_t mul_root(uint32_t x, const uint2 *lo, const uint2 *hi, uint32_t E) {
+    const uint2 a = __ldg(lo + (E & (kLoSize - 1u)));
+    const uint2 b = __ldg(hi + (E >> kLoBits));
+    return norm<Q>(shoup<Q>(shoup<Q>(x, a.x, a.y), b.x, b.y));
 }
-
-__device__ __forceinline__ uint32_t reduce_limb(uint32_t a, uint32_t p) {
-    return (a >= p) ? a - p : a;   // a < 2^32 < 2p
+// R * w^E (Montgomery form of w^E) for E < 2^25, result in [0, p)
+template <int Q>
+__device__ __forceinline__ uint32_t root_m(const uint2 *lo, const uint2 *hi, uint32_t E) {
+    return mul_root<Q>(PrimeC<Q>::r1, lo, hi, E);
 }
-
-// w^E for E < 2^27 (w the table's root), Montgomery form.
-__device__ __forceinline__ uint32_t root_pow(const uint32_t *lo, const uint32_t *hi, uint32_t E,
-                                             uint32_t p, uint32_t pinv) {
-    return mont_mul(__ldg(lo + (E & (kLoSize - 1))), __ldg(hi + (E >> kLoBits)), p, pinv);
+// x * g^(+-E) for E < 2^28, result in [0, p)
+template <int Q>
+__device__ __forceinline__ uint32_t mul_coset(uint32_t x, const uint32_t *lo, const uint32_t *hi, uint32_t E) {
+    const uint32_t a = __ldg(lo + (E & (kCosetSize - 1u)));
+    const uint32_t b = __ldg(hi + (E >> kCosetLoBits));
+    return norm<Q>(mont<Q>(mont<Q>(x, a), b));
 }
 
 __device__ __forceinline__ uint32_t bitrev(uint32_t x, int bits) {
     return bits ? (__brev(x) >> (32 - bits)) : 0u;
 }
+__host__ __device__ constexpr uint32_t crev(uint32_t x, int bits) {
+    uint32_t r = 0u;
+    for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+}
 
 // In-place radix-2 transform of every column of a shared-memory tile
-// T[R][TC] (row-major, R = 2^log_r points per column, TC = 2^log_tc columns).
+// T[R][TC] (row-major, R = 2^log_r points per column, TC = 2^log_tc columns);
+// used for transforms too small for the register-stage kernels.
 // Forward: decimation in frequency, natural order in, bit-reversed order out.
 // Inverse: decimation in time, bit-reversed in, natural out (unscaled).
-// tw[e] = (w_R)^e or (w_R)^-e for e < R/2, Montgomery form, in shared memory.
-template <bool INVERSE>
-__device__ __forceinline__ void tile_transform(uint32_t *T, int log_r, int log_tc,
-                                               const uint32_t *tw, uint32_t p, uint32_t pinv) {
+// tw[e] = (w_R)^(+-e) for e < R/2 with its Shoup companion (the LEVEL table
+// of level log_r - 1).
+template <int Q, bool INVERSE>
+__device__ __forceinline__ void tile_transform(uint32_t *T, int log_r, int log_tc, const uint2 *tw) {
+    constexpr uint32_t P = Prime<Q>::p;
     const uint32_t nb = 1u << (log_r - 1 + log_tc);
     const uint32_t tcmask = (1u << log_tc) - 1u;
     for (int step = 0; step < log_r; ++step) {
@@ -121,28 +205,19 @@ __device__ __forceinline__ void tile_transform(uint32_t *T, int log_r, int log_t
             const uint32_t i1 = i0 + (h << log_tc);
             const uint32_t x = T[i0];
             const uint32_t y = T[i1];
-            const uint32_t w = tw[pos << twshift];
+            const uint2 w = tw[pos << twshift];
             if (!INVERSE) {
-                T[i0] = add_mod(x, y, p);
-                T[i1] = mont_mul(sub_mod(x, y, p), w, p, pinv);
+                T[i0] = add_n<Q>(x, y);
+                T[i1] = norm<Q>(shoup<Q>(x - y + P, w.x, w.y));
             } else {
-                const uint32_t t = mont_mul(y, w, p, pinv);
-                T[i0] = add_mod(x, t, p);
-                T[i1] = sub_mod(x, t, p);
+                const uint32_t t = norm<Q>(shoup<Q>(y, w.x, w.y));
+                T[i0] = add_n<Q>(x, t);
+                T[i1] = sub_n<Q>(x, t);
             }
         }
         __syncthreads();
     }
 }
-
-// Garner: (r0, r1, r2) residues -> 96-bit value (3 limbs).
-struct CrtConsts {
-    uint32_t p0_inv_mod_p1_m;   // (p0^-1 mod p1) in Montgomery form mod p1
-    uint32_t p0_inv_mod_p2_m;
-    uint32_t p1_inv_mod_p2_m;
-    uint64_t p0p1;
-};
-
 
 // ---------------------------------------------------------------------------
 // Register-resident radix-2^B stages (all shapes compile-time).
@@ -178,6 +253,7 @@ struct StagePlan {
 template <int LOG_R, int LOG_TC, int LO, int B>
 struct Stage {
     static constexpr uint32_t T = 1u << (LOG_R + LOG_TC - 4);
+    static constexpr int kB = B, kLO = LO;
     __device__ static __forceinline__ void elem(uint32_t t, int j, uint32_t &pos, uint32_t &c) {
         const int g = j >> B;
         const uint32_t v = (uint32_t)j & ((1u << B) - 1u);
@@ -208,32 +284,45 @@ struct Stage {
             x[j] = S[addr(pos, c)];
         }
     }
-    // tw[e] = w_R^(+/-e), e < R/2
-    template <bool INV>
-    __device__ static __forceinline__ void levels(uint32_t (&x)[16], uint32_t t, const uint32_t *tw, uint32_t p,
-                                                  uint32_t pinv) {
+    // tw = the LEVEL table (levels 0 .. LOG_R - 1).
+    // In a level of half-span h = s*2^lm the butterfly of group element v uses
+    // w_(2h)^(low + s*(v mod 2^lm)): only 2^lm distinct twiddles per group,
+    // loaded once each from the contiguous table of that level, so the lanes
+    // of a warp read consecutive entries or one broadcast entry.  The
+    // half-span-1 level (LO = 0, lm = 0) has twiddle 1 and needs no product.
+    template <bool INV, int Q>
+    __device__ static __forceinline__ void levels(uint32_t (&x)[16], uint32_t t, const uint2 *tw) {
+        constexpr uint32_t P = Prime<Q>::p;
+        constexpr int G = 16 >> B;
 #pragma unroll
         for (int step = 0; step < B; ++step) {
             const int lm = INV ? step : (B - 1 - step);
             const int mm = 1 << lm;
             const int lh = LO + lm;
-            const int shift = LOG_R - 1 - lh;
-            const uint32_t hmask = (1u << lh) - 1u;
+            const uint32_t lbase = (1u << lh) - 1u;
+            const bool trivial = (lh == 0);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                if (j & mm) continue;   // partner j + mm stays inside the 2^B group
-                uint32_t pos, c;
-                elem(t, j, pos, c);
-                const uint32_t w = tw[(pos & hmask) << shift];
-                const uint32_t a = x[j];
-                const uint32_t b = x[j + mm];
-                if (!INV) {
-                    x[j] = add_mod(a, b, p);
-                    x[j + mm] = mont_mul(sub_mod(a, b, p), w, p, pinv);
-                } else {
-                    const uint32_t u = mont_mul(b, w, p, pinv);
-                    x[j] = add_mod(a, u, p);
-                    x[j + mm] = sub_mod(a, u, p);
+            for (int g = 0; g < G; ++g) {
+                uint32_t pos0, c0;
+                elem(t, g << B, pos0, c0);                  // v = 0 of this group
+                const uint32_t low = pos0 & ((1u << LO) - 1u);
+#pragma unroll
+                for (int u = 0; u < mm; ++u) {
+                    const uint2 w = trivial ? make_uint2(1u, 0u) : tw[lbase + low + ((uint32_t)u << LO)];
+#pragma unroll
+                    for (int v = u; v < (1 << B); v += 2 * mm) {
+                        const int j = (g << B) + v;
+                        const uint32_t a = x[j];
+                        const uint32_t b = x[j + mm];
+                        if (!INV) {
+                            x[j] = add_n<Q>(a, b);
+                            x[j + mm] = trivial ? sub_n<Q>(a, b) : norm<Q>(shoup<Q>(a - b + P, w.x, w.y));
+                        } else {
+                            const uint32_t y = trivial ? b : norm<Q>(shoup<Q>(b, w.x, w.y));
+                            x[j] = add_n<Q>(a, y);
+                            x[j + mm] = sub_n<Q>(a, y);
+                        }
+                    }
                 }
             }
         }
@@ -248,10 +337,9 @@ struct ExecStage {
     using S = Stage<LOG_R, LOG_TC, I::LO, I::B>;
 };
 
-// Runs execution stages K .. n-1 on x; S is the shared tile (stage hand-off).
-template <int LOG_R, int LOG_TC, bool INV, int K>
-__device__ __forceinline__ void run_stages(uint32_t (&x)[16], uint32_t *Sm, uint32_t t, const uint32_t *tw,
-                                           uint32_t p, uint32_t pinv) {
+// Runs execution stages K .. n-1 on x; Sm is the shared tile (stage hand-off).
+template <int LOG_R, int LOG_TC, bool INV, int Q, int K>
+__device__ __forceinline__ void run_stages(uint32_t (&x)[16], uint32_t *Sm, uint32_t t, const uint2 *tw) {
     constexpr int n = StagePlan<LOG_R>::n;
     if constexpr (K < n) {
         using Cur = typename ExecStage<LOG_R, LOG_TC, INV, K>::S;
@@ -262,8 +350,8 @@ __device__ __forceinline__ void run_stages(uint32_t (&x)[16], uint32_t *Sm, uint
             Cur::load(Sm, x, t);
             __syncthreads();
         }
-        Cur::template levels<INV>(x, t, tw, p, pinv);
-        run_stages<LOG_R, LOG_TC, INV, K + 1>(x, Sm, t, tw, p, pinv);
+        Cur::template levels<INV, Q>(x, t, tw);
+        run_stages<LOG_R, LOG_TC, INV, Q, K + 1>(x, Sm, t, tw);
     }
 }
 

@@ -105,10 +105,32 @@ def test_uneven_pairs_sample(ctx):
         _check_mul(ctx, 1, La, Lb, La, Lb, La + Lb, rng)
 
 
-def test_ntt_two_cosets(ctx):
-    """Products longer than 2^27 limbs: the residues mod x^K - 1 and
-    x^K - beta^K (K = 2^27) are recombined per coefficient."""
+def test_ntt_cosets(ctx):
+    """Products longer than 2^25 points (the largest transform): M cosets of
+    K = 2^25 points, residues mod x^K - g^(iK), recombined per coefficient
+    through the inverse Vandermonde matrix.  M = 2, 3, 5 and 8 (the limit)."""
     rng = np.random.default_rng(28)
-    L = (1 << 26) + 1
+    La, Lb = (1 << 24) + 7, (1 << 24) + 5                      # M = 2
+    _check_mul(ctx, 1, La, Lb, La, Lb, La + Lb, rng, path="ntt")
+    La, Lb = (1 << 26) + (1 << 24), 5000                       # M = 3, A spans 3 blocks
+    _check_mul(ctx, 1, La, Lb, La, Lb, La + Lb, rng, path="ntt")
+    L = (1 << 26) + 1                                          # M = 5
     _check_mul(ctx, 1, L, L, L, L, 2 * L, rng, path="ntt")
     _check_mul(ctx, 1, L + 1000, L - 999, L + 1000, L - 999, 2 * L + 1, rng, path="ntt", extreme=True)
+    L = 1 << 27                                                # M = 8: need = 2^28 - 1
+    _check_mul(ctx, 1, L, L, L, L, 2 * L, rng, path="ntt", extreme=True)
+
+
+def test_ntt_cosets_broadcast_and_square(ctx):
+    """Coset products with a stride-0 B (transformed once for all rows) and a squaring."""
+    rng = np.random.default_rng(29)
+    N, La, Lb = 2, (1 << 25) - 100, 3000                       # need > 2^25: M = 2
+    A, B, C = rand_buf(rng, N, La, La), rand_buf(rng, 1, Lb, Lb), rand_buf(rng, N, La + Lb, 0)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    ctx.mul_ntt(N, dA.ptr, La, La, dB.ptr, Lb, 0, dC.ptr, La + Lb)
+    assert ref.mul_check(N, A, La, La, B, Lb, 0, dC.numpy(), La + Lb)
+    L = (1 << 24) + 3                                          # squaring, M = 2
+    S = rand_buf(rng, 1, 2 * L, 0)
+    dS = to_dev(S)
+    ctx.mul_ntt(1, dA.ptr, L, L, dA.ptr, L, L, dS.ptr, 2 * L)
+    assert ref.mul_check(1, A, L, L, A, L, L, dS.numpy(), 2 * L)
