@@ -34,6 +34,15 @@ import time
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
+
+# DRAM traffic of the dominant kernel family relative to its algorithmic
+# bytes, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of
+# k_rows_r<12> on a 2^22 x 2^22-limb product: 264.0 MB against 302.0 MB of
+# algorithmic bytes; part of the output is still in L2 at kernel end).  The
+# pi run's launches are scaled by their algorithmic bytes.
+NCU_TRAFFIC_RATIO = {"ntt_rows_fused": 264.006 / 301.990}
+NCU_TRAFFIC_SOURCE = ("ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product, "
+                      "scaled to each launch by its algorithmic bytes")
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ms to 1e9 digits of pi (bit-exact), tuned vs plain form on B200; NTT HBM GB/s"
@@ -168,14 +177,17 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     ctx = g.Context()
     digits = args.digits
-    # warm-up (also sizes the workspace and the stream-ordered pool)
-    for _ in range(args.warmup):
-        g.pi_compute(digits, ctx, device_only=True)
-    torch.cuda.synchronize()
-
-    # device-timed steps, results stay in HBM; kernel timers on for the roofline
+    # warm-up (also sizes the workspace, the stream-ordered pool and, with the
+    # kernel timers on, their event pool)
     g.timer_reset()
     g.timer_enable(True)
+    for _ in range(args.warmup):
+        g.pi_compute(digits, ctx, device_only=True)
+    g.timer_enable(False)
+    g.timer_reset()
+    torch.cuda.synchronize()
+
+    # device-timed steps, results stay in HBM
     clocks = Clocks(local)
     _barrier(ws)
     torch.cuda.synchronize()
@@ -193,20 +205,38 @@ def run_ours(args, ws, rank, local):
     clk = clocks.stop()
     _barrier(ws)
     launches = g.launch_count() - launches0
-    g.timer_enable(False)
-    ktimes = g.timer_report()
     ms_local = e0.elapsed_time(e1) / args.steps
     ms = _max_over_ranks(ms_local, ws)
 
+    # the same steps again with per-launch CUDA events around every kernel
+    # (kernel families and the roofline of the dominant one)
+    g.timer_reset()
+    g.timer_enable(True)
+    _barrier(ws)
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for _ in range(args.steps):
+        g.pi_compute(digits, ctx, device_only=True)
+    e3.record()
+    torch.cuda.synchronize()
+    g.timer_enable(False)
+    ktimes = g.timer_report()
+    ms_timed_local = e2.elapsed_time(e3) / args.steps
+
     # end to end through the C ABI, digits + RET copied to pinned host memory
     pinned = torch.empty(digits, dtype=torch.uint8, pin_memory=True)
+    pinned_ret = torch.empty(g.ret_limbs_bound(digits), dtype=torch.int32, pin_memory=True)
+    # one untimed call first: the first use of freshly pinned pages is slow
+    g.pi_compute(digits, ctx, host_digits=pinned, host_ret=pinned_ret)
     h0, d0 = g.transfer_bytes()
     e2e_times = []
     ret_hash = None
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = g.pi_compute(digits, ctx, host_digits=pinned)
+        r = g.pi_compute(digits, ctx, host_digits=pinned, host_ret=pinned_ret)
         torch.cuda.synchronize()
         e2e_times.append((time.perf_counter() - t0) * 1e3)
     h1, d1 = g.transfer_bytes()
@@ -226,8 +256,12 @@ def run_ours(args, ws, rank, local):
     if dom:
         name, (n, kms, kbytes) = dom
         achieved = kbytes / (kms * 1e-3) / 1e9
+        ratio = NCU_TRAFFIC_RATIO.get(name)
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": (ratio * kbytes / n) if ratio else None,
+                "traffic_unit": "bytes per launch (DRAM read + write)",
+                "traffic_source": NCU_TRAFFIC_SOURCE if ratio else None,
                 "launches_per_step": n / args.steps, "share_of_kernel_time": kms / total_kernel_ms,
                 "peak_source": "measured" if not peaks.get("fallback") else "fallback"}
     families = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
@@ -245,6 +279,7 @@ def run_ours(args, ws, rank, local):
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "working set (tens of GB) larger than L2; no flush needed"},
         "pipeline_elapsed_ms": statistics.mean(inner),
+        "ms_per_step_with_kernel_timers": ms_timed_local,
         "ret_len": r.ret_len, "ret_hash": ret_hash, "convert_digits": r.convert_digits,
         "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": (h1 - h0) // args.steps,
                 "d2h_bytes_per_step": (d1 - d0) // args.steps},

@@ -289,21 +289,32 @@ class PiResult:
         self.leaf_digits = leaf_digits
 
 
+def ret_limbs_bound(digits: int) -> int:
+    """An upper bound on RET's length in limbs for ``digits`` digits."""
+    return (int(digits * 3.322) + 31) // 32 + 8
+
+
 def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None = None,
                ret_capacity: int | None = None, device_only: bool = False, profile: bool = False,
-               host_digits=None) -> PiResult:
+               host_digits=None, host_ret=None) -> PiResult:
     """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional).
 
-    ``host_digits``: optional writable host buffer (e.g. a pinned torch uint8
-    tensor) receiving the digits directly from the device.  ``device_only``
-    keeps RET and the digits on the device (no host copies at all)."""
+    ``host_digits`` / ``host_ret``: optional writable host buffers (e.g. pinned
+    torch tensors: uint8 for the digits, 32-bit for RET, at least
+    ret_limbs_bound(digits) limbs) receiving the digits and RET directly from
+    the device.  ``device_only`` keeps RET and the digits on the device (no
+    host copies at all)."""
     _torch()
     l = lib()
     if copy_digits is None:
         copy_digits = 0 if device_only else digits
-    if ret_capacity is None:
-        ret_capacity = 0 if device_only else (int(digits * 3.322) + 31) // 32 + 8
-    ret = np.zeros(max(ret_capacity, 1), dtype=np.uint32)
+    if host_ret is not None:
+        ret_capacity = host_ret.numel() if hasattr(host_ret, "numel") else len(host_ret)
+        ret = host_ret.numpy().view(np.uint32) if hasattr(host_ret, "numpy") else host_ret
+    else:
+        if ret_capacity is None:
+            ret_capacity = 0 if device_only else ret_limbs_bound(digits)
+        ret = np.empty(max(ret_capacity, 1), dtype=np.uint32)
     if host_digits is not None:
         dptr = host_digits.data_ptr() if hasattr(host_digits, "data_ptr") else ctypes.addressof(host_digits)
         dbuf = None
@@ -319,4 +330,4 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
     elapsed = np.frombuffer(np.uint32(info[2]).tobytes(), dtype=np.float32)[0]
     dec = dbuf.raw[:copy_digits].decode("ascii") if dbuf is not None else ""
     return PiResult(digits, info[0], ret_len, float(elapsed), info[3],
-                    ret[:ret_len].copy() if ret_capacity else None, dec, info[5])
+                    ret[:ret_len] if ret_capacity else None, dec, info[5])

@@ -134,9 +134,13 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
                 uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC);
 bool school_thread_fits(uint32_t La, uint32_t Lb);
 
-// Largest L_a + L_b handled by schoolbook (the reference's crossover is 1024,
-// batch_arith.cu:181).  Overridable for tuning with gpupi_set_mul_crossover().
-static uint32_t g_school_max = 1024u;
+// Largest L_a + L_b handled by schoolbook.  The reference switches at 1024
+// (batch_arith.cu:181); on B200 this library's NTT overtakes its schoolbook
+// kernels between 384 and 512 limbs (batched products of 2^27 limbs in total:
+// 384 -> 3.8 ms school / 4.7 ms NTT, 512 -> 4.6 / 3.7 ms), so the switch is
+// at 448.  The product is exact either way.  Overridable for tuning with
+// gpupi_set_mul_crossover().
+static uint32_t g_school_max = 448u;
 
 }  // namespace gpupi
 

@@ -163,13 +163,11 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
     req.ctx = raw(ctx);
     req.device_only = (flags & 2u) != 0u;
     req.host_digits = h_digits;
+    req.host_ret = h_ret;
+    req.host_ret_cap = h_ret ? ret_cap : 0;
     gpupi::PiOutput out;
     cudaError_t err = gpupi::pi_run(req, out);
     if (err != cudaSuccess) return (int)err;
-    if (h_ret) {
-        const size_t n = std::min<size_t>(ret_cap, out.ret.size());
-        memcpy(h_ret, out.ret.data(), n * 4);
-    }
     if (info) {
         uint32_t leaf = 0u;
         gpupi::round_up_decimal_digits(digits, &leaf);

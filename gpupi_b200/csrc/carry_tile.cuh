@@ -107,14 +107,65 @@ __global__ void carry_fixup_kernel(uint32_t *C, uint64_t sC, uint32_t N, uint32_
     }
 }
 
+// Cross-tile carry fix-up for long rows: one 1024-thread CTA per row walks
+// the row's flags 1024 tiles at a time (block-wide ballot resolution, the
+// next chunk's flags loaded while the current one resolves), so a row of T
+// tiles costs T/1024 dependent steps instead of T/32.
+template <bool SUB>
+__global__ void __launch_bounds__(1024) carry_fixup_rows_kernel(uint32_t *C, uint64_t sC, uint32_t Lc,
+                                                                uint32_t tiles_per_row, uint32_t span,
+                                                                const uint32_t *flags) {
+    __shared__ uint32_t sg[32], sp[32];
+    const uint32_t row = blockIdx.x;
+    const uint32_t *fr = flags + (uint64_t)row * tiles_per_row;
+    uint32_t *out = C + row * sC;
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t wmask = (1u << w) - 1u;
+    uint32_t cin = 0u;
+    uint32_t fnext = (threadIdx.x < tiles_per_row) ? fr[threadIdx.x] : 0u;
+    for (uint32_t base = 0; base < tiles_per_row; base += 1024u) {
+        const uint32_t t = base + threadIdx.x;
+        const uint32_t f = fnext;   // 0 beyond the row: neither generates nor propagates
+        const uint32_t tn = t + 1024u;
+        fnext = (tn < tiles_per_row) ? fr[tn] : 0u;
+        const bool p = ((f >> 1) & 1u) != 0u;
+        const BlockCarry bc = block_resolve<32>((f & 1u) != 0u, p, sg, sp);
+        // carry into this tile when the chunk itself receives cin: every
+        // earlier tile of the chunk must propagate
+        const uint32_t pm = __ballot_sync(0xffffffffu, p);
+        uint32_t wp = 0u;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) wp |= sp[k] << k;
+        const bool prev_all = ((pm & lt) == lt) && ((wp & wmask) == wmask);
+        const uint32_t tin = bc.cin | (prev_all ? cin : 0u);
+        if (t < tiles_per_row && tin) {
+            const uint64_t start = (uint64_t)t * span;
+            const uint32_t pre = f >> 2;
+            for (uint32_t k = 0; k < pre && start + k < Lc; ++k) out[start + k] = SUB ? 0xffffffffu : 0u;
+            if (pre < span && start + pre < Lc)
+                out[start + pre] = SUB ? out[start + pre] - 1u : out[start + pre] + 1u;
+        }
+        cin = bc.G | (bc.P & cin);
+        __syncthreads();   // sg / sp are rewritten by the next chunk
+    }
+}
+
 inline void launch_carry_fixup(bool sub, uint32_t *C, uint64_t sC, uint32_t N, uint32_t Lc,
                                uint32_t tiles_per_row, uint32_t span, const uint32_t *flags,
                                cudaStream_t st) {
-    const unsigned grid = grid_for(N, 4, kNumSMs * 8);
-    if (sub)
-        carry_fixup_kernel<true><<<grid, 128, 0, st>>>(C, sC, N, Lc, tiles_per_row, span, flags);
-    else
-        carry_fixup_kernel<false><<<grid, 128, 0, st>>>(C, sC, N, Lc, tiles_per_row, span, flags);
+    if (tiles_per_row > 64u) {
+        if (sub)
+            carry_fixup_rows_kernel<true><<<N, 1024, 0, st>>>(C, sC, Lc, tiles_per_row, span, flags);
+        else
+            carry_fixup_rows_kernel<false><<<N, 1024, 0, st>>>(C, sC, Lc, tiles_per_row, span, flags);
+    } else {
+        const unsigned grid = grid_for(N, 4, kNumSMs * 8);
+        if (sub)
+            carry_fixup_kernel<true><<<grid, 128, 0, st>>>(C, sC, N, Lc, tiles_per_row, span, flags);
+        else
+            carry_fixup_kernel<false><<<grid, 128, 0, st>>>(C, sC, N, Lc, tiles_per_row, span, flags);
+    }
     count_launch();
 }
 

@@ -102,21 +102,6 @@ struct ColsArgs {
     int M;               // cosets per row
 };
 
-// Residue q of element i (natural order) of coset `coset` of operand row xr:
-// (X mod (x^K - c)) [i] * g^(coset * i), c = g^(coset K) (Montgomery form cm).
-template <int Q>
-__device__ __forceinline__ uint32_t load_operand(const ColsArgs &a, const uint32_t *xr, uint64_t i, uint64_t K,
-                                                 int coset, uint32_t cm, const uint32_t *clo,
-                                                 const uint32_t *chi) {
-    if (a.M == 1) return (i < a.Lx) ? reduce_limb<Q>(__ldg(xr + i)) : 0u;
-    uint32_t acc = 0u;
-    for (int b = (int)a.nb - 1; b >= 0; --b) {   // Horner over the K-limb blocks
-        const uint64_t ii = i + (uint64_t)b * K;
-        const uint32_t xv = (ii < a.Lx) ? reduce_limb<Q>(__ldg(xr + ii)) : 0u;
-        acc = add_n<Q>(coset ? norm<Q>(mont<Q>(acc, cm)) : acc, xv);
-    }
-    return coset ? mul_coset<Q>(acc, clo, chi, (uint32_t)coset * (uint32_t)i) : acc;
-}
 
 // Offset of element j from element 0 in a LO = 0 stage with 2^B-point groups
 // (LOG_R >= 4): j = g 2^B + v sits at pos_0 + v + g 2^(LOG_R - 4 + B), bits
@@ -174,10 +159,21 @@ __device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a,
     const int log_cols = a.log_s - LOG_R;
     const uint32_t ctiles = 1u << (log_cols - LOG_TC);
     const uint32_t nseg = 1u << (a.log_k - a.log_s);
-    const uint32_t ct = (uint32_t)(b % ctiles);
-    b /= ctiles;
-    const uint32_t seg = (uint32_t)(b % nseg);
-    const uint64_t vrow = b / nseg;
+    uint32_t ct, seg;
+    uint64_t vrow;
+    if constexpr (FROM_LIMBS) {
+        // virtual row fastest: the cosets of one tile run back to back and
+        // share its limbs in L2 (the first pass covers the whole transform)
+        const uint64_t vrows = (gridDim.x / kPrimes) / ctiles;
+        vrow = b % vrows;
+        ct = (uint32_t)(b / vrows);
+        seg = 0u;
+    } else {
+        ct = (uint32_t)(b % ctiles);
+        b /= ctiles;
+        seg = (uint32_t)(b % nseg);
+        vrow = b / nseg;
+    }
     const int dir = INVERSE ? 1 : 0;
     const uint64_t K = 1ull << a.log_k;
     const uint2 *twhi = root_hi_ptr(P.tab, dir, Q);
@@ -197,12 +193,60 @@ __device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a,
         const uint32_t *chi = coset_hi_ptr(P.tab, 0, Q);
         // coset node c = g^(coset K), Montgomery form
         const uint32_t cm = (a.M > 1) ? mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << a.log_k) : 0u;
+        if (a.M == 1) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            uint32_t pos, c;
-            First::elem(t, j, pos, c);
-            const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
-            x[j] = load_operand<Q>(a, xr, i, K, coset, cm, clo, chi);
+            for (int j = 0; j < 16; ++j) {
+                uint32_t pos, c;
+                First::elem(t, j, pos, c);
+                const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+                x[j] = (i < a.Lx) ? reduce_limb<Q>(__ldg(xr + i)) : 0u;
+            }
+        } else {
+            // X mod (x^K - c): Horner over the K-limb blocks, top block first,
+            // the 16 loads of a block issued together
+#pragma unroll
+            for (int j = 0; j < 16; ++j) x[j] = 0u;
+            for (int blk = (int)a.nb - 1; blk >= 0; --blk) {
+                uint32_t v[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    uint32_t pos, c;
+                    First::elem(t, j, pos, c);
+                    const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c + (uint64_t)blk * K;
+                    v[j] = (i < a.Lx) ? __ldg(xr + i) : 0u;
+                }
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    x[j] = add_n<Q>(coset ? norm<Q>(mont<Q>(x[j], cm)) : x[j], reduce_limb<Q>(v[j]));
+            }
+        }
+        if (coset) {
+            // twist by g^(coset i).  For LOG_R >= 4 the 16 residues of a thread
+            // sit at i_0 + v 2^(LO + log_cols) (one group), so the factors are
+            // g^(coset i_0) D^v with D = g^(coset 2^(LO + log_cols)), the same for
+            // the whole CTA: two lookup pairs and fifteen products.
+            if constexpr (LOG_R >= 4) {
+                static_assert(First::kB == 4, "one group per thread");
+                uint32_t pos, c;
+                First::elem(t, 0, pos, c);
+                const uint32_t i0 = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
+                uint32_t f = mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset * i0);
+                const uint32_t d =
+                    mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << (First::kLO + log_cols));
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    x[j] = norm<Q>(mont<Q>(x[j], f));
+                    f = mont<Q>(f, d);   // lazy, < 2p
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    uint32_t pos, c;
+                    First::elem(t, j, pos, c);
+                    const uint32_t i = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
+                    x[j] = mul_coset<Q>(x[j], clo, chi, (uint32_t)coset * i);
+                }
+            }
         }
     } else {
 #pragma unroll
@@ -322,7 +366,7 @@ constexpr size_t rows_smem_bytes() {
 }
 
 template <int LOG_C, bool FROM_LIMBS>
-__global__ void __launch_bounds__((1 << LOG_C) / 16) k_rows_r(NttParams P, RowsArgs a) {
+__global__ void __launch_bounds__((1 << LOG_C) / 16, LOG_C == 12 ? 4 : 1) k_rows_r(NttParams P, RowsArgs a) {
     extern __shared__ uint4 rows_smem[];
     constexpr int C = 1 << LOG_C;
     uint32_t *Sm = reinterpret_cast<uint32_t *>(rows_smem);
@@ -496,24 +540,40 @@ __device__ __forceinline__ void crt_chunk(const uint32_t *F0, int log_k, uint32_
 
 __global__ void __launch_bounds__(kThreads) k_crt(CrtArgs a) {
     __shared__ uint32_t sg[kThreads / 32], sp[kThreads / 32], spre[kThreads / 32];
+    __shared__ uint32_t spill[kThreads / 32][3];
     const uint32_t tile = blockIdx.x;
     const uint64_t row = tile / a.tiles;
     const uint32_t t = tile - (uint32_t)row * a.tiles;
     const uint64_t K = 1ull << a.log_k;
     const uint32_t *F0 = a.F + row * (uint64_t)a.M * 3 * K;
     const int64_t base = (int64_t)t * kCrtSpan + threadIdx.x * kCrtV;
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     uint32_t S[kCrtV + 3];
     crt_chunk(F0, a.log_k, a.Lc - 1u, base, S);
+    // words of the previous chunk's sum that land in this chunk: from the
+    // previous lane, from the previous warp's last lane, and for the tile's
+    // first thread from the last chunk of the previous tile (recomputed)
     uint32_t H[3];
     H[0] = __shfl_up_sync(0xffffffffu, S[kCrtV], 1);
     H[1] = __shfl_up_sync(0xffffffffu, S[kCrtV + 1], 1);
     H[2] = __shfl_up_sync(0xffffffffu, S[kCrtV + 2], 1);
-    if (lane_id() == 0) {
+    if (lane == 31) {
+        spill[warp][0] = S[kCrtV];
+        spill[warp][1] = S[kCrtV + 1];
+        spill[warp][2] = S[kCrtV + 2];
+    }
+    if (threadIdx.x == 0) {
         uint32_t Sp[kCrtV + 3];
         crt_chunk(F0, a.log_k, a.Lc - 1u, base - kCrtV, Sp);
         H[0] = Sp[kCrtV];
         H[1] = Sp[kCrtV + 1];
         H[2] = Sp[kCrtV + 2];
+    }
+    __syncthreads();
+    if (lane == 0 && warp > 0) {
+        H[0] = spill[warp - 1][0];
+        H[1] = spill[warp - 1][1];
+        H[2] = spill[warp - 1][2];
     }
     uint32_t X[kCrtV];
     const uint32_t g = chunk_add_spill<kCrtV>(S, H, X);

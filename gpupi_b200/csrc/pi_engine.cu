@@ -749,6 +749,21 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     ConvertDecimalPowerTable powers{};
     char *d_digits = nullptr;
     if (err == cudaSuccess) err = pi_fractional(ctx, &prof, (int)requested, retb, RET);
+    // RET into the caller's buffer on a side stream, overlapping the decimal
+    // conversion (which only reads RET)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ret_ready = nullptr;
+    if (err == cudaSuccess && !req.device_only && req.host_ret && RET.length) {
+        const size_t n = std::min<size_t>(req.host_ret_cap, RET.length);
+        err = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&ret_ready, cudaEventDisableTiming);
+        if (err == cudaSuccess) err = cudaEventRecord(ret_ready, st);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(side, ret_ready, 0);
+        if (err == cudaSuccess && n) {
+            err = cudaMemcpyAsync(req.host_ret, RET.data, n * 4, cudaMemcpyDeviceToHost, side);
+            note_d2h(n * 4);
+        }
+    }
     if (err == cudaSuccess) {
         err = stage(&prof, "decimal_powers", "precompute_5pow", levels == 0u ? leaf : (leaf << levels), 1u, levels,
                     leaf, false, [&]() { return convert_decimal_precompute_powers(ctx, &powers, leaf, levels); });
@@ -770,8 +785,8 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     out.ret_len = RET.length;
     out.workspace_bytes = batch_mp_workspace_size(ctx);
     if (err == cudaSuccess && !req.device_only) {
-        out.ret.resize(RET.length);
-        if (RET.length) {
+        if (!req.host_ret) out.ret.resize(RET.length);
+        if (RET.length && !req.host_ret) {
             err = cudaMemcpyAsync(out.ret.data(), RET.data, (size_t)RET.length * 4, cudaMemcpyDeviceToHost, st);
             note_d2h((size_t)RET.length * 4);
         }
@@ -793,6 +808,12 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
         }
         if (err == cudaSuccess) err = cudaStreamSynchronize(st);
     }
+    if (side) {
+        const cudaError_t serr = cudaStreamSynchronize(side);
+        if (err == cudaSuccess) err = serr;
+        cudaStreamDestroy(side);
+    }
+    if (ret_ready) cudaEventDestroy(ret_ready);
     out.stages = prof.entries;
     if (d_digits) cudaFreeAsync(d_digits, st);
     convert_decimal_release_powers(&powers);

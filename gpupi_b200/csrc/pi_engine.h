@@ -25,6 +25,8 @@ struct PiRequest {
     BatchMPContext *ctx = nullptr;  // reuse a context (keeps its workspace); null = private
     bool device_only = false;       // leave RET and the digits on the device (no host copies)
     char *host_digits = nullptr;    // caller buffer (>= copy_digits bytes, may be pinned) for the digits
+    uint32_t *host_ret = nullptr;   // caller buffer for RET (copied while the digits are converted)
+    size_t host_ret_cap = 0;        // its capacity in limbs
 };
 
 struct PiOutput {

@@ -91,8 +91,9 @@ int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *d_X, uint32_t L_x, uin
 
 /* Whole pi_bs_gpu pipeline (pi_bs_gpu.cu:2073-2431, main_fractional).
  * h_ret (capacity ret_cap limbs) receives RET, h_digits (capacity digits_cap)
- * the first min(digits, digits_cap) decimal digits after "3." (copied
- * straight from the device; pinned memory makes that copy fastest).  Either
+ * the first min(digits, digits_cap) decimal digits after "3."; both are
+ * copied straight from the device (RET while the digits are still being
+ * converted), so pinned memory makes those copies fastest.  Either
  * may be null.  info[0..7] receives: convert_digits, RET length, elapsed ms
  * on the device (float bits), workspace MB, number of profiled stages, leaf
  * digits, 0, 0.  flags bit 0 = profile every stage, bit 1 = keep RET and the

@@ -87,7 +87,7 @@ def test_broadcast_and_square(ctx):
     assert np.array_equal(dS.numpy(), ref.mul(1, A, La, La, A, La, La, S, 2 * La))
 
 
-@pytest.mark.parametrize("L", [510, 511, 512, 513, 1023, 1024, 1025])
+@pytest.mark.parametrize("L", [447, 448, 449, 510, 511, 512, 513, 1023, 1024, 1025])
 def test_crossover_boundary(ctx, L):
     """Products on both sides of the schoolbook/NTT crossover (batch_arith_test.cu:98-102)."""
     rng = np.random.default_rng(L)

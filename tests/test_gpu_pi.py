@@ -36,3 +36,18 @@ def test_pi_golden(ctx, entry):
     assert r.convert_digits == entry["convert_digits"]
     assert hashlib.sha256(r.dec.encode()).hexdigest() == entry["dec_sha256"]
     assert pi_ref.decimal_hash(r.dec[:4096]) == entry["dec_preview_hash"]
+
+
+@pytest.mark.parametrize("digits", [1000, 1000000])
+def test_pi_into_pinned_buffers(ctx, digits):
+    """RET and the digits copied straight into caller-owned pinned buffers
+    (RET on a side stream while the digits are converted) match the default path."""
+    import torch
+    import gpupi_b200 as g
+    want = g.pi_compute(digits, ctx)
+    hd = torch.zeros(digits, dtype=torch.uint8, pin_memory=True)
+    hr = torch.zeros(g.ret_limbs_bound(digits), dtype=torch.int32, pin_memory=True)
+    r = g.pi_compute(digits, ctx, host_digits=hd, host_ret=hr)
+    assert r.ret_len == want.ret_len
+    assert np.array_equal(r.ret, want.ret)
+    assert bytes(hd.numpy()).decode() == want.dec
