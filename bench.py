@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import random
 import time
 from pathlib import Path
 
@@ -40,6 +41,7 @@ ROOT = Path(__file__).resolve().parent
 # k_rows_r<12> on a 2^22 x 2^22-limb product: 264.0 MB against 302.0 MB of
 # algorithmic bytes; part of the output is still in L2 at kernel end).  The
 # pi run's launches are scaled by their algorithmic bytes.
+BBP_POSITIONS = 64
 NCU_TRAFFIC_RATIO = {"ntt_rows_fused": 264.006 / 301.990}
 NCU_TRAFFIC_SOURCE = ("ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product, "
                       "scaled to each launch by its algorithmic bytes")
@@ -248,6 +250,19 @@ def run_ours(args, ws, rank, local):
     ret_hash = mod_hash(r.ret)
     e2e = _max_over_ranks(statistics.mean(e2e_times), ws)
 
+    # independent check of RET: BBP hex digits at 64 seeded positions
+    # (integer fixed point on the GPU), outside the timed regions
+    bbp = None
+    if rank == 0:
+        rng = random.Random(0xBB964)
+        top = 8 * (r.ret_len - 1) - 64
+        positions = sorted(rng.randrange(0, top) for _ in range(BBP_POSITIONS))
+        t0 = time.perf_counter()
+        bad, unsure = g.bbp_spot_check(r.ret, positions)
+        bbp = {"positions": len(positions), "hex_digits_each": 6, "mismatches": len(bad),
+               "inconclusive": len(unsure), "seconds": round(time.perf_counter() - t0, 2),
+               "max_position": positions[-1]}
+
     # roofline of the dominant kernel family
     peaks = _peaks()
     dom = max(ktimes.items(), key=lambda kv: kv[1][1]) if ktimes else None
@@ -288,6 +303,7 @@ def run_ours(args, ws, rank, local):
         "kernel_families": families,
         "clocks": clk,
         "cpu_baseline": cpu,
+        "bbp_check": bbp,
     }
     print(json.dumps(line), flush=True)
     ctx.close()

@@ -63,6 +63,7 @@ _SIGS = [
     ("gpupi_transfer_bytes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     ("gpupi_mp_add_noalloc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
     ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
+    ("gpupi_bbp_fractions", ctypes.c_int, [_p, _u32, _p]),
 ]
 
 C_ABI_SYMBOLS = [s[0] for s in _SIGS]
@@ -331,3 +332,51 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
     dec = dbuf.raw[:copy_digits].decode("ascii") if dbuf is not None else ""
     return PiResult(digits, info[0], ret_len, float(elapsed), info[3],
                     ret[:ret_len] if ret_capacity else None, dec, info[5])
+
+
+# ---------------------------------------------------------------------------
+# BBP spot check of RET (independent of the binary-splitting pipeline)
+# ---------------------------------------------------------------------------
+def bbp_fractions(positions) -> np.ndarray:
+    """floor(2^64 frac(16^n pi)) for each n in ``positions`` (0-based: n = 0
+    gives the hex digits right after the point), computed on the GPU with
+    integer fixed point; each value is within 8 (n + 17) units of exact."""
+    _torch()
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.uint64))
+    out = np.zeros(len(pos), dtype=np.uint64)
+    if len(pos):
+        _check(lib().gpupi_bbp_fractions(pos.ctypes.data, len(pos), out.ctypes.data), "gpupi_bbp_fractions")
+    return out
+
+
+def ret_hex_bits(ret, n: int, bits: int = 24) -> int:
+    """The ``bits`` bits of pi starting 4n bits below the point, read from
+    RET (little-endian limbs, pi * 2^(32 (len - 1)) truncated: the top limb is
+    the integer part 3, the next one holds hex digits 1..8)."""
+    L = len(ret)
+    top = 32 * (L - 1) - 4 * n      # bit index just above the window
+    lo = top - bits
+    if lo < 0:
+        raise ValueError("position beyond RET")
+    val = 0
+    for i in range(lo // 32, (top - 1) // 32 + 1):
+        val |= int(ret[i]) << (32 * i)
+    return (val >> lo) & ((1 << bits) - 1)
+
+
+def bbp_spot_check(ret, positions, bits: int = 24):
+    """Compare ``bits`` bits of RET at each position with the BBP fraction.
+    Returns (mismatches, inconclusive): a position is inconclusive when the
+    BBP error bound could move the compared bits."""
+    fr = bbp_fractions(positions)
+    bad, unsure = [], []
+    shift = 64 - bits
+    for n, f in zip(positions, fr):
+        f = int(f)
+        err = 8 * (int(n) + 17)
+        lo, hi = ((f - err) % (1 << 64)) >> shift, ((f + err) % (1 << 64)) >> shift
+        if lo != hi:
+            unsure.append(int(n))
+        elif ret_hex_bits(ret, int(n), bits) != (f >> shift):
+            bad.append(int(n))
+    return bad, unsure

@@ -15,6 +15,10 @@ struct gpupi_ctx {
     BatchMPContext *ctx;
 };
 
+namespace gpupi {
+cudaError_t bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *fractions);
+}
+
 namespace {
 inline BatchMPArray view(const uint32_t *d, uint32_t len, uint32_t n, uint32_t stride) {
     return BatchMPArray{const_cast<uint32_t *>(d), len, n, stride};
@@ -194,6 +198,10 @@ int gpupi_timer_reset(void) {
 }
 
 size_t gpupi_timer_report(char *buf, size_t cap) { return gpupi::kernel_timer_report(buf, cap); }
+
+int gpupi_bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *fractions) {
+    return (int)gpupi::bbp_fractions(positions, count, fractions);
+}
 
 int gpupi_transfer_bytes(uint64_t *h2d, uint64_t *d2h) {
     gpupi::transfer_bytes(h2d, d2h);

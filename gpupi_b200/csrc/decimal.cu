@@ -223,17 +223,30 @@ static std::vector<uint32_t> pow5(uint32_t e) {
     return v;
 }
 
+// Stream-ordered scratch buffer (no device-wide synchronisation on free).
 struct DevBuf {
     uint32_t *p = nullptr;
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, current_stream());
     }
     cudaError_t alloc(size_t words) {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, current_stream());
         p = nullptr;
-        return words ? cudaMalloc(&p, words * 4) : cudaSuccess;
+        return words ? cudaMallocAsync((void **)&p, words * 4, current_stream()) : cudaSuccess;
     }
 };
+
+// One row of the power table, from the stream-ordered pool.
+BatchMPArray power_array(uint32_t length) {
+    BatchMPArray a{nullptr, length, 1u, length};
+    if (length && cudaMallocAsync((void **)&a.data, (size_t)length * 4, current_stream()) != cudaSuccess)
+        a = BatchMPArray{};
+    return a;
+}
+void power_release(BatchMPArray &a) {
+    if (a.data) cudaFreeAsync(a.data, current_stream());
+    a = BatchMPArray{};
+}
 
 }  // namespace gpupi
 
@@ -256,12 +269,12 @@ cudaError_t convert_decimal_precompute_powers(BatchMPContext *ctx, ConvertDecima
     if (powers == nullptr) return cudaErrorMemoryAllocation;
     for (uint32_t i = 0; i < levels; ++i) powers[i] = BatchMPArray{};
     auto fail = [&](uint32_t made, cudaError_t e) {
-        for (uint32_t i = 0; i < made; ++i) batch_mp_array_release(powers[i]);
+        for (uint32_t i = 0; i < made; ++i) power_release(powers[i]);
         delete[] powers;
         return e;
     };
     const std::vector<uint32_t> base = pow5(leaf_digits);
-    powers[0] = batch_mp_array_create(1u, (uint32_t)base.size());
+    powers[0] = power_array((uint32_t)base.size());
     if (powers[0].data == nullptr) return fail(0, cudaErrorMemoryAllocation);
     cudaError_t err = cudaMemcpyAsync(powers[0].data, base.data(), base.size() * 4,
                                       cudaMemcpyHostToDevice, current_stream());
@@ -269,12 +282,12 @@ cudaError_t convert_decimal_precompute_powers(BatchMPContext *ctx, ConvertDecima
     if (err == cudaSuccess) err = cudaStreamSynchronize(current_stream());
     if (err != cudaSuccess) return fail(1, err);
     for (uint32_t l = 1; l < levels; ++l) {
-        BatchMPArray next = batch_mp_array_create(1u, powers[l - 1].length * 2u);
+        BatchMPArray next = power_array(powers[l - 1].length * 2u);
         if (next.data == nullptr) return fail(l, cudaErrorMemoryAllocation);
         err = batch_mp_mul(ctx, powers[l - 1], powers[l - 1], next);
         if (err == cudaSuccess) err = next.compact(ctx);
         if (err != cudaSuccess) {
-            batch_mp_array_release(next);
+            power_release(next);
             return fail(l, err);
         }
         powers[l] = next;
@@ -287,7 +300,7 @@ cudaError_t convert_decimal_precompute_powers(BatchMPContext *ctx, ConvertDecima
 void convert_decimal_release_powers(ConvertDecimalPowerTable *table) {
     if (table == nullptr) return;
     if (table->powers != nullptr) {
-        for (uint32_t i = 0; i < table->levels; ++i) batch_mp_array_release(table->powers[i]);
+        for (uint32_t i = 0; i < table->levels; ++i) power_release(table->powers[i]);
         delete[] table->powers;
     }
     table->powers = nullptr;

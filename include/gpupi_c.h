@@ -129,6 +129,14 @@ int gpupi_mp_add_noalloc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t
 /* Multiply crossover: largest L_a + L_b computed by schoolbook (<= 1024). */
 int gpupi_set_mul_crossover(uint32_t max_school_len);
 
+/* BBP spot check of pi's hex digits, independent of the binary-splitting
+ * pipeline (the north-star C5 check; no counterpart in the reference).
+ * fractions[i] = floor(2^64 * frac(16^positions[i] * pi)) up to an error of
+ * at most 8 * (positions[i] + 17) units (integer fixed point, host arrays),
+ * so hex digits positions[i] + 1, ... of pi can be compared with RET where
+ * that bound cannot flip them.  positions[i] <= 2^30. */
+int gpupi_bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *fractions);
+
 #ifdef __cplusplus
 }
 #endif
