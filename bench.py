@@ -79,6 +79,15 @@ class Clocks:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi's own start-up (NVML initialisation) must not fall inside
+        # the timed region: wait for its first sample before timing starts
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            self.f.flush()
+            if self.path.exists() and self.path.stat().st_size > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -191,10 +200,10 @@ def run_ours(args, ws, rank, local):
 
     # device-timed steps, results stay in HBM
     clocks = Clocks(local)
+    clocks.start()
     _barrier(ws)
     torch.cuda.synchronize()
     launches0 = g.launch_count()
-    clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()

@@ -100,8 +100,13 @@ struct ColsArgs {
     uint32_t *F;         // workspace of this operand: F[vrow][q][K]
     int log_k, log_s;
     int M;               // cosets per row
+    // second operand of a paired forward pass (same shape, same tile)
+    const uint32_t *X2;
+    uint64_t sX2;
+    uint32_t Lx2;
+    uint32_t nb2;
+    uint32_t *F2;
 };
-
 
 // Offset of element j from element 0 in a LO = 0 stage with 2^B-point groups
 // (LOG_R >= 4): j = g 2^B + v sits at pos_0 + v + g 2^(LOG_R - 4 + B), bits
@@ -112,14 +117,15 @@ __host__ __device__ constexpr uint32_t stage_delta(int j, int B, int log_r) {
 
 // Twist the 16 residues of stage S (the LO = 0 stage: last forward, first
 // inverse) by w_S^(col * bitrev(pos)) or its inverse, E = colsh * bitrev(pos)
-// with colsh = col << shift.  For LOG_R >= 4 the column is the same for all
-// 16 residues and bitrev(pos_j) = bitrev(pos_0) + sum over the set bits i of
-// j of bitrev(delta_(2^i)), so the 16 factors are the subset products of
-// w^(E_0) and four D_i = w^(colsh bitrev(delta_(2^i))): five table lookups
-// and fifteen products instead of sixteen scattered lookup pairs.
-template <class S, int LOG_R, int Q>
-__device__ __forceinline__ void twist16(uint32_t (&x)[16], uint32_t t, uint32_t c0, int shift, const uint2 *lo,
-                                        const uint2 *hi) {
+// with colsh = col << shift; with PAIR the same factors twist y as well.
+// For LOG_R >= 4 the column is the same for all 16 residues and
+// bitrev(pos_j) = bitrev(pos_0) + sum over the set bits i of j of
+// bitrev(delta_(2^i)), so the 16 factors are the subset products of w^(E_0)
+// and four D_i = w^(colsh bitrev(delta_(2^i))): five table lookups and
+// fifteen products instead of sixteen scattered lookup pairs.
+template <class S, int LOG_R, int Q, bool PAIR>
+__device__ __forceinline__ void twist16(uint32_t (&x)[16], uint32_t (&y)[16], uint32_t t, uint32_t c0, int shift,
+                                        const uint2 *lo, const uint2 *hi) {
     if constexpr (LOG_R >= 4) {
         constexpr int B = S::kB;
         static_assert(S::kLO == 0, "twist stage");
@@ -135,23 +141,91 @@ __device__ __forceinline__ void twist16(uint32_t (&x)[16], uint32_t t, uint32_t 
             for (int k = 0; k < (1 << i); ++k) F[(1 << i) + k] = mont<Q>(F[k], D);   // lazy, < 2p
         }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(x[j], F[j]));
+        for (int j = 0; j < 16; ++j) {
+            x[j] = norm<Q>(mont<Q>(x[j], F[j]));
+            if (PAIR) y[j] = norm<Q>(mont<Q>(y[j], F[j]));
+        }
     } else {
         // short columns: the 16 residues span several columns
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             uint32_t pos, c;
             S::elem(t, j, pos, c);
-            x[j] = mul_root<Q>(x[j], lo, hi, ((c0 + c) << shift) * bitrev(pos, LOG_R));
+            const uint32_t E = ((c0 + c) << shift) * bitrev(pos, LOG_R);
+            x[j] = mul_root<Q>(x[j], lo, hi, E);
+            if (PAIR) y[j] = mul_root<Q>(y[j], lo, hi, E);
+        }
+    }
+}
+
+// The 16 first-pass residues of one operand (limbs, folded into coset
+// `coset` and twisted by g^(coset i) when the row is split into cosets).
+template <class First, int LOG_R, int Q>
+__device__ __forceinline__ void load_limbs(const ColsArgs &a, uint32_t (&x)[16], const uint32_t *xr, uint32_t Lx,
+                                           uint32_t nb, uint64_t K, int log_cols, uint32_t c0, uint32_t t,
+                                           int coset, uint32_t cm, const uint32_t *clo, const uint32_t *chi) {
+    if (a.M == 1) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+            x[j] = (i < Lx) ? reduce_limb<Q>(__ldg(xr + i)) : 0u;
+        }
+        return;
+    }
+    // X mod (x^K - c): Horner over the K-limb blocks, top block first, the
+    // 16 loads of a block issued together
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = 0u;
+    for (int blk = (int)nb - 1; blk >= 0; --blk) {
+        uint32_t v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c + (uint64_t)blk * K;
+            v[j] = (i < Lx) ? __ldg(xr + i) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            x[j] = add_n<Q>(coset ? norm<Q>(mont<Q>(x[j], cm)) : x[j], reduce_limb<Q>(v[j]));
+    }
+    if (coset) {
+        // twist by g^(coset i).  For LOG_R >= 4 the 16 residues of a thread sit
+        // at i_0 + v 2^(LO + log_cols) (one group), so the factors are
+        // g^(coset i_0) D^v with D = g^(coset 2^(LO + log_cols)), the same for
+        // the whole CTA: two lookup pairs and fifteen products.
+        if constexpr (LOG_R >= 4) {
+            static_assert(First::kB == 4, "one group per thread");
+            uint32_t pos, c;
+            First::elem(t, 0, pos, c);
+            const uint32_t i0 = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
+            uint32_t f = mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset * i0);
+            const uint32_t d = mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << (First::kLO + log_cols));
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                x[j] = norm<Q>(mont<Q>(x[j], f));
+                f = mont<Q>(f, d);   // lazy, < 2p
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                uint32_t pos, c;
+                First::elem(t, j, pos, c);
+                const uint32_t i = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
+                x[j] = mul_coset<Q>(x[j], clo, chi, (uint32_t)coset * i);
+            }
         }
     }
 }
 
 // Column pass: R = 2^LOG_R (<= 512) points per column, TC = 4096 / R columns
-// per CTA; segment of S = 2^log_s points viewed as [R][S/R].
-template <int LOG_R, bool FROM_LIMBS, bool INVERSE, int Q>
+// per CTA; segment of S = 2^log_s points viewed as [R][S/R].  PAIR: the
+// forward pass of A and B together (same tile, shared twiddles and twists).
+template <int LOG_R, bool FROM_LIMBS, bool INVERSE, bool PAIR, int Q>
 __device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a, uint64_t b, uint32_t *Sm,
-                                          uint2 *tw) {
+                                          uint32_t *Sm2, uint2 *tw) {
     constexpr int LOG_TC = 12 - LOG_R;
     constexpr int NS = StagePlan<LOG_R>::n;
     using First = typename ExecStage<LOG_R, LOG_TC, INVERSE, 0>::S;
@@ -180,106 +254,61 @@ __device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a,
     const uint2 *twlo = root_lo_ptr(P.tab, dir, Q);
     const uint2 *lev = level_ptr(P.tab, dir, Q);
     for (uint32_t e = threadIdx.x; e < (1u << LOG_R) - 1u; e += kThreads) tw[e] = __ldg(lev + e);
-    uint32_t *F = a.F + vrow * 3 * K + (uint64_t)Q * K + ((uint64_t)seg << a.log_s);
+    const uint64_t off = vrow * 3 * K + (uint64_t)Q * K + ((uint64_t)seg << a.log_s);
+    uint32_t *F = a.F + off;
+    uint32_t *F2 = PAIR ? a.F2 + off : nullptr;
     const uint32_t c0 = ct << LOG_TC;
     const int twist_shift = kMaxLog - a.log_s;
     const uint32_t t = threadIdx.x;
-    uint32_t x[16];
+    uint32_t x[16], y[16];
     if constexpr (FROM_LIMBS) {
         const uint64_t row = vrow / (uint32_t)a.M;
         const int coset = (int)(vrow - row * (uint32_t)a.M);
-        const uint32_t *xr = a.X + row * a.sX;
         const uint32_t *clo = coset_lo_ptr(P.tab, 0, Q);
         const uint32_t *chi = coset_hi_ptr(P.tab, 0, Q);
         // coset node c = g^(coset K), Montgomery form
         const uint32_t cm = (a.M > 1) ? mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << a.log_k) : 0u;
-        if (a.M == 1) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                uint32_t pos, c;
-                First::elem(t, j, pos, c);
-                const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
-                x[j] = (i < a.Lx) ? reduce_limb<Q>(__ldg(xr + i)) : 0u;
-            }
-        } else {
-            // X mod (x^K - c): Horner over the K-limb blocks, top block first,
-            // the 16 loads of a block issued together
-#pragma unroll
-            for (int j = 0; j < 16; ++j) x[j] = 0u;
-            for (int blk = (int)a.nb - 1; blk >= 0; --blk) {
-                uint32_t v[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    uint32_t pos, c;
-                    First::elem(t, j, pos, c);
-                    const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c + (uint64_t)blk * K;
-                    v[j] = (i < a.Lx) ? __ldg(xr + i) : 0u;
-                }
-#pragma unroll
-                for (int j = 0; j < 16; ++j)
-                    x[j] = add_n<Q>(coset ? norm<Q>(mont<Q>(x[j], cm)) : x[j], reduce_limb<Q>(v[j]));
-            }
-        }
-        if (coset) {
-            // twist by g^(coset i).  For LOG_R >= 4 the 16 residues of a thread
-            // sit at i_0 + v 2^(LO + log_cols) (one group), so the factors are
-            // g^(coset i_0) D^v with D = g^(coset 2^(LO + log_cols)), the same for
-            // the whole CTA: two lookup pairs and fifteen products.
-            if constexpr (LOG_R >= 4) {
-                static_assert(First::kB == 4, "one group per thread");
-                uint32_t pos, c;
-                First::elem(t, 0, pos, c);
-                const uint32_t i0 = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
-                uint32_t f = mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset * i0);
-                const uint32_t d =
-                    mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << (First::kLO + log_cols));
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    x[j] = norm<Q>(mont<Q>(x[j], f));
-                    f = mont<Q>(f, d);   // lazy, < 2p
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    uint32_t pos, c;
-                    First::elem(t, j, pos, c);
-                    const uint32_t i = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
-                    x[j] = mul_coset<Q>(x[j], clo, chi, (uint32_t)coset * i);
-                }
-            }
-        }
+        load_limbs<First, LOG_R, Q>(a, x, a.X + row * a.sX, a.Lx, a.nb, K, log_cols, c0, t, coset, cm, clo, chi);
+        if constexpr (PAIR)
+            load_limbs<First, LOG_R, Q>(a, y, a.X2 + row * a.sX2, a.Lx2, a.nb2, K, log_cols, c0, t, coset, cm, clo,
+                                        chi);
     } else {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             uint32_t pos, c;
             First::elem(t, j, pos, c);
-            x[j] = F[((uint64_t)pos << log_cols) + c0 + c];
+            const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+            x[j] = F[i];
+            if constexpr (PAIR) y[j] = F2[i];
         }
-        if constexpr (INVERSE) twist16<First, LOG_R, Q>(x, t, c0, twist_shift, twlo, twhi);
+        if constexpr (INVERSE) twist16<First, LOG_R, Q, PAIR>(x, y, t, c0, twist_shift, twlo, twhi);
     }
     __syncthreads();   // twiddle table ready
-    run_stages<LOG_R, LOG_TC, INVERSE, Q, 0>(x, Sm, t, tw);
-    if constexpr (!INVERSE) twist16<Last, LOG_R, Q>(x, t, c0, twist_shift, twlo, twhi);
+    run_stages_pair<LOG_R, LOG_TC, INVERSE, Q, 0, PAIR>(x, y, Sm, Sm2, t, tw);
+    if constexpr (!INVERSE) twist16<Last, LOG_R, Q, PAIR>(x, y, t, c0, twist_shift, twlo, twhi);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         uint32_t pos, c;
         Last::elem(t, j, pos, c);
-        F[((uint64_t)pos << log_cols) + c0 + c] = x[j];
+        const uint64_t i = ((uint64_t)pos << log_cols) + c0 + c;
+        F[i] = x[j];
+        if constexpr (PAIR) F2[i] = y[j];
     }
 }
 
-template <int LOG_R, bool FROM_LIMBS, bool INVERSE>
-__global__ void __launch_bounds__(kThreads) k_cols_r(NttParams P, ColsArgs a) {
-    __shared__ uint32_t Sm[kTilePad];
+template <int LOG_R, bool FROM_LIMBS, bool INVERSE, bool PAIR>
+__global__ void __launch_bounds__(kThreads, PAIR ? 3 : 4) k_cols_r(NttParams P, ColsArgs a) {
+    __shared__ uint32_t Sm[PAIR ? 2 * kTilePad : kTilePad];
     __shared__ uint2 tw[(1 << LOG_R) - 1];
+    uint32_t *Sm2 = PAIR ? Sm + kTilePad : Sm;
     uint64_t b;
     const int q = grid_prime(b);
     if (q == 0)
-        cols_body<LOG_R, FROM_LIMBS, INVERSE, 0>(P, a, b, Sm, tw);
+        cols_body<LOG_R, FROM_LIMBS, INVERSE, PAIR, 0>(P, a, b, Sm, Sm2, tw);
     else if (q == 1)
-        cols_body<LOG_R, FROM_LIMBS, INVERSE, 1>(P, a, b, Sm, tw);
+        cols_body<LOG_R, FROM_LIMBS, INVERSE, PAIR, 1>(P, a, b, Sm, Sm2, tw);
     else
-        cols_body<LOG_R, FROM_LIMBS, INVERSE, 2>(P, a, b, Sm, tw);
+        cols_body<LOG_R, FROM_LIMBS, INVERSE, PAIR, 2>(P, a, b, Sm, Sm2, tw);
 }
 
 struct RowsArgs {
@@ -340,6 +369,7 @@ __device__ __forceinline__ void rows_body(const NttParams &P, const RowsArgs &a,
     run_stages<LOG_C, 0, false, Q, 0>(xa, Sm, t, tw);
     if (!a.square) {
         // the tile is free again: every thread has passed the last stage's loads
+        // (A and B one after the other: a second tile would cost a CTA per SM)
         __syncthreads();
         run_stages<LOG_C, 0, false, Q, 0>(xb, Sm, t, tw);
     }
@@ -361,7 +391,7 @@ __device__ __forceinline__ void rows_body(const NttParams &P, const RowsArgs &a,
 }
 
 template <int LOG_C>
-constexpr size_t rows_smem_bytes() {
+constexpr size_t rows_smem_bytes() {   // the padded tile + the twiddle levels
     return (size_t)((1 << LOG_C) + (1 << LOG_C) / 32) * 4u + (size_t)((1 << LOG_C) - 1) * 8u;
 }
 
@@ -622,38 +652,57 @@ static Shape shape_for(uint32_t La, uint32_t Lb) {
     return {kMaxLog, (int)((need + K - 1) / K)};
 }
 
-template <bool FL, bool INV>
+// Paired passes exist for R >= 32 only (shorter columns twist per residue
+// and would spill with two operands).
+constexpr int kPairMinLogR = 5;
+
+template <bool FL, bool INV, bool PAIR>
 static void cols_r_dispatch(int log_r, unsigned blocks, const NttParams &P, const ColsArgs &a, cudaStream_t st) {
+    if constexpr (!PAIR) {
+        switch (log_r) {
+            case 1: k_cols_r<1, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
+            case 2: k_cols_r<2, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
+            case 3: k_cols_r<3, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
+            case 4: k_cols_r<4, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
+            default: break;
+        }
+    }
     switch (log_r) {
-        case 1: k_cols_r<1, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 2: k_cols_r<2, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 3: k_cols_r<3, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 4: k_cols_r<4, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 5: k_cols_r<5, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 6: k_cols_r<6, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 7: k_cols_r<7, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 8: k_cols_r<8, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
-        default: k_cols_r<9, FL, INV><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 5: k_cols_r<5, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 6: k_cols_r<6, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 7: k_cols_r<7, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 8: k_cols_r<8, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
+        default: k_cols_r<9, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
     }
 }
 
-static void launch_cols_r(bool from_limbs, bool inverse, int log_r, const NttParams &P, const ColsArgs &a,
-                          uint64_t vrows, cudaStream_t st) {
+// One column pass over vrows virtual rows (pair: operands A and B together).
+static void launch_cols_r(bool from_limbs, bool inverse, bool pair, int log_r, const NttParams &P,
+                          const ColsArgs &a, uint64_t vrows, cudaStream_t st) {
     const uint64_t ctiles = 1ull << (a.log_s - 12);
     const uint64_t nseg = 1ull << (a.log_k - a.log_s);
     const unsigned blocks = (unsigned)(vrows * kPrimes * nseg * ctiles);
-    // algorithmic bytes: 12 B per point (3 primes x 4 B) read and written;
-    // the first pass reads the limbs instead (once per coset)
+    // algorithmic bytes: 4 B per residue read and written (3 primes per
+    // point); the first pass reads the limbs instead (once per coset)
     const double K = (double)(1ull << a.log_k);
-    const double bytes = from_limbs ? (4.0 * a.Lx * (double)vrows / a.M + 12.0 * K * (double)vrows)
-                                    : 24.0 * K * (double)vrows;
+    const double limbs = (double)a.Lx + (pair ? (double)a.Lx2 : 0.0);
+    const double ops = pair ? 2.0 : 1.0;
+    const double bytes = from_limbs ? (4.0 * limbs * (double)vrows / a.M + 12.0 * K * (double)vrows * ops)
+                                    : 24.0 * K * (double)vrows * ops;
     KernelTimed kt(from_limbs ? "ntt_cols_fwd_first" : (inverse ? "ntt_cols_inv" : "ntt_cols_fwd"), bytes);
-    if (from_limbs)
-        cols_r_dispatch<true, false>(log_r, blocks, P, a, st);
-    else if (!inverse)
-        cols_r_dispatch<false, false>(log_r, blocks, P, a, st);
-    else
-        cols_r_dispatch<false, true>(log_r, blocks, P, a, st);
+    if (from_limbs) {
+        if (pair)
+            cols_r_dispatch<true, false, true>(log_r, blocks, P, a, st);
+        else
+            cols_r_dispatch<true, false, false>(log_r, blocks, P, a, st);
+    } else if (!inverse) {
+        if (pair)
+            cols_r_dispatch<false, false, true>(log_r, blocks, P, a, st);
+        else
+            cols_r_dispatch<false, false, false>(log_r, blocks, P, a, st);
+    } else {
+        cols_r_dispatch<false, true, false>(log_r, blocks, P, a, st);
+    }
     count_launch();
 }
 
@@ -788,18 +837,21 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
             passes[1] = rest / 2;
             npass = 2;
         }
-        // forward column passes for A and (unless squaring) B
-        for (int op = 0; op < (square ? 1 : 2); ++op) {
+        // forward column passes: A and B together (one launch per pass) unless
+        // B is A or a broadcast row
+        const bool pair = !square && !bcast && passes[0] >= kPairMinLogR && (npass == 1 || passes[1] >= kPairMinLogR);
+        for (int op = 0; op < (pair || square ? 1 : 2); ++op) {
             const uint32_t *X = op == 0 ? A : B;
             const uint64_t sX = op == 0 ? sA : sB;
             const uint32_t Lx = op == 0 ? La : Lb;
             uint32_t *F = op == 0 ? FA : FB;
             const uint64_t vrows = (op == 1 && bcast) ? (uint64_t)M : VR;
             const uint32_t nb = (uint32_t)((Lx + K - 1) / K);
+            const uint32_t nb2 = (uint32_t)((Lb + K - 1) / K);
             int log_s = log_k;
             for (int ps = 0; ps < npass; ++ps) {
-                ColsArgs a{X, sX, Lx, nb, F, log_k, log_s, M};
-                launch_cols_r(ps == 0, false, passes[ps], P, a, vrows, st);
+                ColsArgs a{X, sX, Lx, nb, F, log_k, log_s, M, pair ? B : nullptr, sB, Lb, nb2, pair ? FB : nullptr};
+                launch_cols_r(ps == 0, false, pair, passes[ps], P, a, vrows, st);
                 log_s -= passes[ps];
             }
         }
@@ -814,8 +866,8 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         int log_s = log_c;
         for (int ps = npass - 1; ps >= 0; --ps) {
             log_s += passes[ps];
-            ColsArgs a{nullptr, 0, 0, 0, FA, log_k, log_s, M};
-            launch_cols_r(false, true, passes[ps], P, a, VR, st);
+            ColsArgs a{nullptr, 0, 0, 0, FA, log_k, log_s, M, nullptr, 0, 0, 0, nullptr};
+            launch_cols_r(false, true, false, passes[ps], P, a, VR, st);
         }
         if (M > 1) {
             CombineArgs c{};

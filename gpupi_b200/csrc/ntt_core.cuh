@@ -291,8 +291,28 @@ struct Stage {
     // of a warp read consecutive entries or one broadcast entry.  The
     // half-span-1 level (LO = 0, lm = 0) has twiddle 1 and needs no product.
     template <bool INV, int Q>
-    __device__ static __forceinline__ void levels(uint32_t (&x)[16], uint32_t t, const uint2 *tw) {
+    __device__ static __forceinline__ void bfly(uint32_t (&x)[16], int j, int mm, uint2 w, bool trivial) {
         constexpr uint32_t P = Prime<Q>::p;
+        const uint32_t a = x[j];
+        const uint32_t b = x[j + mm];
+        if (!INV) {
+            x[j] = add_n<Q>(a, b);
+            x[j + mm] = trivial ? sub_n<Q>(a, b) : norm<Q>(shoup<Q>(a - b + P, w.x, w.y));
+        } else {
+            const uint32_t y = trivial ? b : norm<Q>(shoup<Q>(b, w.x, w.y));
+            x[j] = add_n<Q>(a, y);
+            x[j + mm] = sub_n<Q>(a, y);
+        }
+    }
+    template <bool INV, int Q>
+    __device__ static __forceinline__ void levels(uint32_t (&x)[16], uint32_t t, const uint2 *tw) {
+        levels_pair<INV, Q, false>(x, x, t, tw);
+    }
+    // Two independent transforms of the same shape (PAIR): every twiddle is
+    // loaded once and serves both.
+    template <bool INV, int Q, bool PAIR>
+    __device__ static __forceinline__ void levels_pair(uint32_t (&x)[16], uint32_t (&y)[16], uint32_t t,
+                                                       const uint2 *tw) {
         constexpr int G = 16 >> B;
 #pragma unroll
         for (int step = 0; step < B; ++step) {
@@ -311,17 +331,8 @@ struct Stage {
                     const uint2 w = trivial ? make_uint2(1u, 0u) : tw[lbase + low + ((uint32_t)u << LO)];
 #pragma unroll
                     for (int v = u; v < (1 << B); v += 2 * mm) {
-                        const int j = (g << B) + v;
-                        const uint32_t a = x[j];
-                        const uint32_t b = x[j + mm];
-                        if (!INV) {
-                            x[j] = add_n<Q>(a, b);
-                            x[j + mm] = trivial ? sub_n<Q>(a, b) : norm<Q>(shoup<Q>(a - b + P, w.x, w.y));
-                        } else {
-                            const uint32_t y = trivial ? b : norm<Q>(shoup<Q>(b, w.x, w.y));
-                            x[j] = add_n<Q>(a, y);
-                            x[j + mm] = sub_n<Q>(a, y);
-                        }
+                        bfly<INV, Q>(x, (g << B) + v, mm, w, trivial);
+                        if (PAIR) bfly<INV, Q>(y, (g << B) + v, mm, w, trivial);
                     }
                 }
             }
@@ -337,22 +348,31 @@ struct ExecStage {
     using S = Stage<LOG_R, LOG_TC, I::LO, I::B>;
 };
 
-// Runs execution stages K .. n-1 on x; Sm is the shared tile (stage hand-off).
-template <int LOG_R, int LOG_TC, bool INV, int Q, int K>
-__device__ __forceinline__ void run_stages(uint32_t (&x)[16], uint32_t *Sm, uint32_t t, const uint2 *tw) {
+// Runs execution stages K .. n-1 on x (and, with PAIR, in lockstep on y);
+// Sx / Sy are the shared tiles of the stage hand-offs.
+template <int LOG_R, int LOG_TC, bool INV, int Q, int K, bool PAIR>
+__device__ __forceinline__ void run_stages_pair(uint32_t (&x)[16], uint32_t (&y)[16], uint32_t *Sx, uint32_t *Sy,
+                                                uint32_t t, const uint2 *tw) {
     constexpr int n = StagePlan<LOG_R>::n;
     if constexpr (K < n) {
         using Cur = typename ExecStage<LOG_R, LOG_TC, INV, K>::S;
         if constexpr (K > 0) {
             using Prev = typename ExecStage<LOG_R, LOG_TC, INV, K - 1>::S;
-            Prev::store(Sm, x, t);
+            Prev::store(Sx, x, t);
+            if (PAIR) Prev::store(Sy, y, t);
             __syncthreads();
-            Cur::load(Sm, x, t);
+            Cur::load(Sx, x, t);
+            if (PAIR) Cur::load(Sy, y, t);
             __syncthreads();
         }
-        Cur::template levels<INV, Q>(x, t, tw);
-        run_stages<LOG_R, LOG_TC, INV, Q, K + 1>(x, Sm, t, tw);
+        Cur::template levels_pair<INV, Q, PAIR>(x, y, t, tw);
+        run_stages_pair<LOG_R, LOG_TC, INV, Q, K + 1, PAIR>(x, y, Sx, Sy, t, tw);
     }
+}
+
+template <int LOG_R, int LOG_TC, bool INV, int Q, int K>
+__device__ __forceinline__ void run_stages(uint32_t (&x)[16], uint32_t *Sm, uint32_t t, const uint2 *tw) {
+    run_stages_pair<LOG_R, LOG_TC, INV, Q, K, false>(x, x, Sm, Sm, t, tw);
 }
 
 }  // namespace ntt
