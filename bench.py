@@ -48,8 +48,9 @@ NCU_TRAFFIC_SOURCE = ("ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ms to 1e9 digits of pi (bit-exact), tuned vs plain form on B200; NTT HBM GB/s"
-CPU_SAMPLE_DIGITS = 1_000_000          # ~18 s on one host core
-REF_SAMPLE_DIGITS = 200_000            # per reference-arm step, ~1.5 s
+CPU_SAMPLE_DIGITS = 20_000_000         # host C++ restatement, all cores: ~9 s on 8 cores
+REF_SAMPLE_DIGITS = 10_000_000         # per reference-arm step, ~4 s on 8 cores
+PY_SAMPLE_DIGITS = 1_000_000           # CPython fallback when the C++ restatement is not built
 
 
 def _peaks() -> dict:
@@ -139,43 +140,91 @@ def _barrier(ws: int):
         dist.barrier()
 
 
+def _pi_cpu(digits: int) -> dict | None:
+    """Run the host C++ restatement (oracle/_build/pi_cpu, GMP, all host
+    threads) once; None when it is not built."""
+    exe = ROOT / "oracle" / "_build" / "pi_cpu"
+    if not exe.exists():
+        return None
+    out = subprocess.run([str(exe), str(digits)], capture_output=True, text=True, check=True).stdout
+    first = out.splitlines()[0]
+    fields = dict(kv.split("=", 1) for kv in first.split() if "=" in kv)
+    ret_hash = int(out.splitlines()[1].rsplit("=", 1)[1])
+    return {"ms": float(fields["elapsed_ms"]), "threads": int(fields["threads"]), "ret_hash": ret_hash}
+
+
+def _cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline_sample(digits: int) -> dict:
+    r = _pi_cpu(digits)
+    if r is not None:
+        ms = r["ms"]
+        return {"value": ms * (1e9 / digits), "unit": "ms (linear extrapolation to 1e9 digits)",
+                "cores": r["threads"], "kind": "port",
+                "sample": f"pi to {digits} digits with the host C++ restatement of the pipeline "
+                          f"(oracle/pi_cpu.cpp, GMP integers, {r['threads']} threads on {_cpu_model()}): "
+                          f"{ms:.1f} ms, RET hash {r['ret_hash']}, scaled by 1e9/{digits} "
+                          f"(a lower bound: binary splitting grows faster than linearly)",
+                "sample_ms": ms}
     sys.path.insert(0, str(ROOT / "oracle"))
     import pi_ref
+    d = PY_SAMPLE_DIGITS
     t0 = time.perf_counter()
-    pi_ref.pi_digits(digits)
+    pi_ref.pi_digits(d)
     ms = (time.perf_counter() - t0) * 1e3
-    return {"value": ms * (1e9 / digits), "unit": "ms (linear extrapolation to 1e9 digits)", "cores": 1,
+    return {"value": ms * (1e9 / d), "unit": "ms (linear extrapolation to 1e9 digits)", "cores": 1,
             "kind": "port",
-            "sample": f"pi to {digits} digits with the CPU restatement of the pipeline (oracle/pi_ref.py, "
-                      f"CPython big integers, one core): {ms:.1f} ms, scaled by 1e9/{digits} "
+            "sample": f"pi to {d} digits with the CPU restatement of the pipeline (oracle/pi_ref.py, "
+                      f"CPython big integers, one core): {ms:.1f} ms, scaled by 1e9/{d} "
                       f"(a lower bound: binary splitting grows faster than linearly)",
             "sample_ms": ms}
 
 
 def run_reference_arm(args, ws, rank):
+    """The reference has no CPU implementation of the pipeline; its arm times
+    the host C++ restatement (GMP, all host threads), the same recurrence and
+    the same RET, on a bounded sample per step scaled to the metric."""
     if rank != 0:
         return
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pi_ref
     d = REF_SAMPLE_DIGITS
-    for _ in range(args.warmup):
-        pi_ref.pi_digits(d)
-    times = []
-    for _ in range(args.steps):
+    use_cpp = _pi_cpu(1000) is not None
+    if not use_cpp:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pi_ref
+        d = PY_SAMPLE_DIGITS // 5
+
+    def one():
+        if use_cpp:
+            return _pi_cpu(d)
         t0 = time.perf_counter()
         pi_ref.pi_digits(d)
-        times.append((time.perf_counter() - t0) * 1e3)
-    ms = statistics.mean(times) * (args.digits / d)
+        return {"ms": (time.perf_counter() - t0) * 1e3, "threads": 1}
+
+    for _ in range(args.warmup):
+        one()
+    runs = [one() for _ in range(args.steps)]
+    ms = statistics.mean(r["ms"] for r in runs) * (args.digits / d)
+    cores = runs[0]["threads"]
+    what = (f"oracle/pi_cpu.cpp (GMP, {cores} threads on {_cpu_model()})" if use_cpp
+            else "oracle/pi_ref.py (CPython, one core)")
     line = {
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (pi has no input data)",
         "config": {"workload": f"pi to {args.digits} digits", "sample_digits_per_step": d,
                    "l2": "inputs larger than L2"},
-        "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
-                         "sample": f"pi to {d} digits per step with oracle/pi_ref.py (the reference has no CPU "
-                                   f"implementation), mean of {args.steps} steps scaled linearly to {args.digits}"},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
+                         "sample": f"pi to {d} digits per step with {what} (the reference has no CPU "
+                                   f"implementation), mean of {args.steps} steps scaled linearly to "
+                                   f"{args.digits} (a lower bound)"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -355,6 +404,42 @@ def run_ntt(args, ws, rank, local):
     ctx.close()
 
 
+def run_convert(args, ws, rank, local):
+    """Decimal conversion of a seeded 2^25-limb binary fraction (2^30 input
+    bits) to 308 * 2^20 = 322,961,408 digits (leaf 308, 20 levels), input
+    and digits resident in HBM."""
+    import torch
+    import gpupi_b200 as g
+
+    torch.cuda.set_device(local)
+    ctx = g.Context()
+    L = 1 << 25
+    leaf, levels = 308, 20
+    total = leaf << levels
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0xC4)
+    X = torch.randint(-2 ** 31, 2 ** 31 - 1, (L,), dtype=torch.int32, device="cuda", generator=gen)
+    out = torch.empty(total, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        ctx.convert_decimal(X.data_ptr(), L, 32 * L, total, leaf, out.data_ptr())
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        ctx.convert_decimal(X.data_ptr(), L, 32 * L, total, leaf, out.data_ptr())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
+    head = bytes(out[:16].cpu().numpy())
+    if rank == 0:
+        print(json.dumps({"metric": f"ms to convert a {L}-limb fraction to {total} decimal digits", "value": ms,
+                          "unit": "ms", "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
+                          "digits_per_s": total / (ms * 1e-3), "first_digits": head.decode("ascii", "replace")}),
+              flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -363,8 +448,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--digits", type=int, default=1_000_000_000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", choices=["pi", "ntt"], default="pi",
-                    help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step")
+    ap.add_argument("--workload", choices=["pi", "ntt", "convert"], default="pi",
+                    help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step; "
+                         "convert: one 2^25-limb decimal conversion per step")
     ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -379,6 +465,8 @@ def main():
             run_reference_arm(args, ws, rank)
         elif args.workload == "ntt":
             run_ntt(args, ws, rank, local)
+        elif args.workload == "convert":
+            run_convert(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

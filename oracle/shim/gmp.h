@@ -1,5 +1,6 @@
-/* Declarations of the GMP 6 public functions the reference sources call
- * (the image ships libgmp.so.10 without its development header).  Names and
+/* Declarations of the GMP 6 public functions the reference sources and the
+ * host C++ restatement (oracle/pi_cpu.cpp) call (the image ships
+ * libgmp.so.10 without its development header).  Names and
  * signatures follow GMP's documented API; the library itself is linked by
  * path.  Used only to build the parity oracle. */
 #ifndef GPUPI_ORACLE_GMP_SHIM_H
@@ -42,6 +43,11 @@ void __gmpz_divexact_ui(mpz_ptr, mpz_srcptr, unsigned long);
 void __gmpz_ui_pow_ui(mpz_ptr, unsigned long, unsigned long);
 size_t __gmpz_sizeinbase(mpz_srcptr, int);
 int __gmpz_cmp(mpz_srcptr, mpz_srcptr);
+int __gmpz_cmp_ui(mpz_srcptr, unsigned long);
+void __gmpz_neg(mpz_ptr, mpz_srcptr);
+void __gmpz_swap(mpz_ptr, mpz_ptr);
+char *__gmpz_get_str(char *, int, mpz_srcptr);
+unsigned long __gmpz_fdiv_ui(mpz_srcptr, unsigned long);
 int __gmp_printf(const char *, ...);
 
 #define mpz_init __gmpz_init
@@ -68,6 +74,11 @@ int __gmp_printf(const char *, ...);
 #define mpz_ui_pow_ui __gmpz_ui_pow_ui
 #define mpz_sizeinbase __gmpz_sizeinbase
 #define mpz_cmp __gmpz_cmp
+#define mpz_cmp_ui __gmpz_cmp_ui
+#define mpz_neg __gmpz_neg
+#define mpz_swap __gmpz_swap
+#define mpz_get_str __gmpz_get_str
+#define mpz_fdiv_ui __gmpz_fdiv_ui
 #define gmp_printf __gmp_printf
 #ifdef __cplusplus
 }

@@ -51,3 +51,18 @@ def test_pi_into_pinned_buffers(ctx, digits):
     assert r.ret_len == want.ret_len
     assert np.array_equal(r.ret, want.ret)
     assert bytes(hd.numpy()).decode() == want.dec
+
+
+def test_pi_1e7_matches_cpp_restatement(ctx):
+    """10^7 digits: RET and every digit equal the host C++ restatement
+    (oracle/pi_cpu.cpp, GMP), built on the spot with g++."""
+    import subprocess
+    import build_cpu
+    import gpupi_b200 as g
+    d = 10_000_000
+    out = subprocess.run([str(build_cpu.build()), str(d)], capture_output=True, text=True,
+                         check=True).stdout.splitlines()
+    r = g.pi_compute(d, ctx)
+    assert f"RET_len={r.ret_len}" in out[0]
+    assert out[1] == pi_ref.hex_preview("RET", r.ret)
+    assert out[3] == f"DEC_hash = {pi_ref.decimal_hash(r.dec)}"

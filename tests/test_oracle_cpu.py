@@ -100,3 +100,19 @@ def test_batch_ref_semantics():
     assert list(q) == [3, 0]
     out = ref.decimal_naive(1, np.array([1 << 31], dtype=np.uint32), 1, 1, 6, 6, bytearray(6))
     assert bytes(out) == b"000005"   # 1/2 -> "500000" written least significant first
+
+
+def test_cpp_restatement_matches_python():
+    """The host C++ restatement (oracle/pi_cpu.cpp, GMP, threads) prints the
+    same RET preview, hash and digits as the Python restatement."""
+    import subprocess
+    import build_cpu
+    exe = build_cpu.build()
+    for d in (0, 100, 20000):
+        out = subprocess.run([str(exe), str(d)], capture_output=True, text=True, check=True).stdout.splitlines()
+        r = pi_ref.pi_digits(d)
+        limbs = pi_ref.to_limbs(r.ret, r.ret_len)
+        assert f"RET_len={r.ret_len}" in out[0]
+        assert out[1] == pi_ref.hex_preview("RET", limbs)
+        if d:
+            assert out[2] == "DEC = 3" + r.digits[:min(63, d)] + "..." + r.digits[d - min(64, d):d]
