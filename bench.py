@@ -440,6 +440,66 @@ def run_convert(args, ws, rank, local):
     ctx.close()
 
 
+def run_uneven(args, ws, rank, local):
+    """4096 independent products with lengths log-uniform in [8, 4096] limbs
+    per operand (seeded), operands resident in HBM: one ragged call
+    (bucketed: schoolbook launch + NTT per transform size) against one
+    batch_mp_mul call per pair, the form gpupi's API allows."""
+    import numpy as np
+    import torch
+    import gpupi_b200 as g
+
+    torch.cuda.set_device(local)
+    ctx = g.Context()
+    rng = np.random.default_rng(0xC2)
+    n = 4096
+    La = np.floor(2 ** rng.uniform(3, 12, size=n)).astype(np.uint32)
+    Lb = np.floor(2 ** rng.uniform(3, 12, size=n)).astype(np.uint32)
+    offA = np.concatenate([[0], np.cumsum(La.astype(np.uint64))[:-1]]).astype(np.uint64)
+    offB = np.concatenate([[0], np.cumsum(Lb.astype(np.uint64))[:-1]]).astype(np.uint64)
+    Lc = La.astype(np.uint64) + Lb
+    offC = np.concatenate([[0], np.cumsum(Lc)[:-1]]).astype(np.uint64)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0xC2)
+    A = torch.randint(-2 ** 31, 2 ** 31 - 1, (int(La.sum()),), dtype=torch.int32, device="cuda", generator=gen)
+    B = torch.randint(-2 ** 31, 2 ** 31 - 1, (int(Lb.sum()),), dtype=torch.int32, device="cuda", generator=gen)
+    C = torch.zeros(int(Lc.sum()), dtype=torch.int32, device="cuda")
+    C2 = torch.zeros_like(C)
+
+    def ragged():
+        ctx.mul_ragged(A.data_ptr(), offA, La, B.data_ptr(), offB, Lb, C.data_ptr(), offC)
+
+    def per_pair():
+        for i in range(n):
+            ctx.mul(1, A.data_ptr() + 4 * int(offA[i]), int(La[i]), int(La[i]),
+                    B.data_ptr() + 4 * int(offB[i]), int(Lb[i]), int(Lb[i]),
+                    C2.data_ptr() + 4 * int(offC[i]), int(Lc[i]), int(Lc[i]))
+
+    def timed(f):
+        for _ in range(args.warmup):
+            f()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_r = _max_over_ranks(timed(ragged), ws)
+    ms_p = _max_over_ranks(timed(per_pair), ws)
+    same = bool(torch.equal(C, C2))
+    if rank == 0:
+        print(json.dumps({"metric": "ms for 4096 uneven products (log-uniform 8..4096 limbs per operand)",
+                          "value": ms_r, "unit": "ms", "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
+                          "plain_per_pair_ms": ms_p, "speedup_vs_per_pair": ms_p / ms_r,
+                          "limb_products": int((La.astype(np.uint64) * Lb).sum()), "results_equal": same}),
+              flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,9 +508,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--digits", type=int, default=1_000_000_000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", choices=["pi", "ntt", "convert"], default="pi",
+    ap.add_argument("--workload", choices=["pi", "ntt", "convert", "uneven"], default="pi",
                     help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step; "
-                         "convert: one 2^25-limb decimal conversion per step")
+                         "convert: one 2^25-limb decimal conversion per step; uneven: 4096 uneven products")
     ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -467,6 +527,8 @@ def main():
             run_ntt(args, ws, rank, local)
         elif args.workload == "convert":
             run_convert(args, ws, rank, local)
+        elif args.workload == "uneven":
+            run_uneven(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

@@ -64,6 +64,7 @@ _SIGS = [
     ("gpupi_mp_add_noalloc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
     ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
     ("gpupi_bbp_fractions", ctypes.c_int, [_p, _u32, _p]),
+    ("gpupi_mp_mul_ragged", ctypes.c_int, [_p, _u32, _p, _p, _p, _p, _p, _p, _p, _p]),
 ]
 
 C_ABI_SYMBOLS = [s[0] for s in _SIGS]
@@ -214,6 +215,16 @@ class Context:
         r = _u32(0)
         _check(lib().gpupi_mp_limblength_max(self.h, N, A, La, sA, ctypes.byref(r)), "batch_mp_limblength_max")
         return r.value
+
+    def mul_ragged(self, A, offA, La, B, offB, Lb, C, offC):
+        """Ragged batch: product i = A[offA[i]:+La[i]] * B[offB[i]:+Lb[i]] into
+        C[offC[i]:+La[i]+Lb[i]] (device pointers A, B, C; host sequences for the
+        offsets and lengths)."""
+        n = len(La)
+        oa, ob, oc = (np.ascontiguousarray(np.asarray(x, dtype=np.uint64)) for x in (offA, offB, offC))
+        la, lb = (np.ascontiguousarray(np.asarray(x, dtype=np.uint32)) for x in (La, Lb))
+        _check(lib().gpupi_mp_mul_ragged(self.h, n, A, oa.ctypes.data, la.ctypes.data, B, ob.ctypes.data,
+                                         lb.ctypes.data, C, oc.ctypes.data), "gpupi_mp_mul_ragged")
 
     def mul_ntt(self, N, A, La, sA, B, Lb, sB, C, sC):
         _check(lib().gpupi_mul_ntt(self.h, N, A, La, sA, B, Lb, sB, C, sC), "batch_mul_ntt")

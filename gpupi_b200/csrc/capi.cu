@@ -17,6 +17,9 @@ struct gpupi_ctx {
 
 namespace gpupi {
 cudaError_t bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *fractions);
+cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const uint64_t *offA, const uint32_t *La,
+                       const uint32_t *B, const uint64_t *offB, const uint32_t *Lb, uint32_t *C,
+                       const uint64_t *offC);
 }
 
 namespace {
@@ -125,6 +128,12 @@ int gpupi_mul_naive(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, con
     batch_mul_naive(const_cast<uint32_t *>(A), const_cast<uint32_t *>(B), C, (int)N, (int)La, (int)Lb, (int)sA,
                     (int)sB, (int)sC);
     return (int)cudaGetLastError();
+}
+
+int gpupi_mp_mul_ragged(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, const uint64_t *offA, const uint32_t *La,
+                        const uint32_t *B, const uint64_t *offB, const uint32_t *Lb, uint32_t *C,
+                        const uint64_t *offC) {
+    return (int)gpupi::mul_ragged(raw(ctx), N, A, offA, La, B, offB, Lb, C, offC);
 }
 
 int gpupi_mul_ntt(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,

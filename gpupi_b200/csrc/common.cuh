@@ -59,6 +59,13 @@ struct KernelTimed {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// One product of a ragged batch: operand offsets and lengths (limbs) and the
+// offset of its L_a + L_b output limbs.
+struct RaggedRow {
+    uint64_t offA, offB, offC;
+    uint32_t La, Lb;
+};
+
 // ---------------------------------------------------------------------------
 // Binary carry resolution across a warp.
 //

@@ -122,21 +122,26 @@ __global__ void __launch_bounds__(32 * kWarpProducts) k_school_warp(const uint32
     }
 }
 
+// rows: optional per-product descriptors (ragged batches); null = uniform
+// La, Lb and strides.
 template <int kSchoolThreads>
 __global__ void __launch_bounds__(kSchoolThreads) k_school_cols(const uint32_t *__restrict__ A,
                                                                 const uint32_t *__restrict__ B,
                                                                 uint32_t *__restrict__ C, uint32_t N,
-                                                                uint32_t La, uint32_t Lb, uint64_t sA,
-                                                                uint64_t sB, uint64_t sC) {
+                                                                uint32_t La_u, uint32_t Lb_u, uint64_t sA,
+                                                                uint64_t sB, uint64_t sC,
+                                                                const RaggedRow *__restrict__ rows) {
     // a[0..La), bpad[j + kPad] = b_j (zero outside [0, Lb))
     __shared__ uint32_t sa[kSchoolMaxL];
     __shared__ uint32_t sb[kSchoolMaxL + kSchoolMaxL + 8];
     __shared__ uint32_t sg[kSchoolThreads / 32], sp[kSchoolThreads / 32];
-    const uint32_t kPad = La + 4;
-    const uint32_t Lc = La + Lb;
     for (uint32_t row = blockIdx.x; row < N; row += gridDim.x) {
-        const uint32_t *ar = A + row * sA;
-        const uint32_t *br = B + row * sB;
+        const RaggedRow d = rows ? rows[row] : RaggedRow{row * sA, row * sB, row * sC, La_u, Lb_u};
+        const uint32_t La = d.La, Lb = d.Lb;
+        const uint32_t kPad = La + 4;
+        const uint32_t Lc = La + Lb;
+        const uint32_t *ar = A + d.offA;
+        const uint32_t *br = B + d.offB;
         for (uint32_t i = threadIdx.x; i < La; i += blockDim.x) sa[i] = ar[i];
         for (uint32_t j = threadIdx.x; j < kPad + Lb + 8; j += blockDim.x)
             sb[j] = (j >= kPad && j - kPad < Lb) ? br[j - kPad] : 0u;
@@ -182,7 +187,7 @@ __global__ void __launch_bounds__(kSchoolThreads) k_school_cols(const uint32_t *
         for (int v = 0; v < kSchoolV; ++v) p = p && (X[v] == 0xffffffffu);
         const BlockCarry bc = block_resolve<kSchoolThreads / 32>(g != 0u, p, sg, sp);
         chunk_increment<kSchoolV>(X, bc.cin);
-        uint32_t *cr = C + row * sC;
+        uint32_t *cr = C + d.offC;
 #pragma unroll
         for (int v = 0; v < kSchoolV; ++v)
             if (k0 + v < Lc) cr[k0 + v] = X[v];
@@ -233,13 +238,24 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
         // one CTA per product, 4 output columns per thread
         const uint32_t g = grid_for(N, 1, kNumSMs * 16);
         if (La + Lb <= 256u)
-            k_school_cols<64><<<g, 64, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+            k_school_cols<64><<<g, 64, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
         else if (La + Lb <= 512u)
-            k_school_cols<128><<<g, 128, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+            k_school_cols<128><<<g, 128, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
         else
-            k_school_cols<256><<<g, 256, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+            k_school_cols<256><<<g, 256, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
         count_launch();
     }
+}
+
+// Ragged batch: rows[i] gives the operands' offsets and lengths (L_a >= L_b,
+// L_a + L_b <= 1024) and the output offset of product i (L_a + L_b limbs).
+void school_mul_ragged(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, const RaggedRow *rows,
+                       uint64_t limb_products) {
+    if (N == 0u) return;
+    cudaStream_t st = current_stream();
+    KernelTimed kt("schoolbook", 8.0 * (double)limb_products);
+    k_school_cols<256><<<grid_for(N, 1, kNumSMs * 16), 256, 0, st>>>(A, B, C, N, 0u, 0u, 0u, 0u, 0u, rows);
+    count_launch();
 }
 
 }  // namespace gpupi

@@ -80,6 +80,16 @@ int gpupi_mul_naive(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stri
 int gpupi_mul_ntt(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
                   const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t stride_C);
 
+/* Ragged batch (no counterpart in the reference, whose batches share one
+ * L_a / L_b): product i = A[offA[i] .. + L_a[i]) * B[offB[i] .. + L_b[i]) into
+ * C[offC[i] .. + L_a[i] + L_b[i]).  d_A, d_B, d_C are device pointers; the
+ * offset and length arrays are host arrays of N entries.  Products are bucketed
+ * (schoolbook in one launch, NTT per transform size) so N uneven products cost
+ * a few launches instead of N calls.  L_a[i] + L_b[i] <= 2^28. */
+int gpupi_mp_mul_ragged(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, const uint64_t *offA, const uint32_t *L_a,
+                        const uint32_t *d_B, const uint64_t *offB, const uint32_t *L_b, uint32_t *d_C,
+                        const uint64_t *offC);
+
 /* batch_decimal_naive (batch_decimal_naive.h:23-31): LSD-first ASCII digits */
 int gpupi_decimal_naive(uint32_t N, const uint32_t *d_A, uint32_t L_limb, uint32_t stride_A, char *d_out,
                         uint32_t L_dec, uint32_t stride_out);

@@ -134,3 +134,40 @@ def test_ntt_cosets_broadcast_and_square(ctx):
     dS = to_dev(S)
     ctx.mul_ntt(1, dA.ptr, L, L, dA.ptr, L, L, dS.ptr, 2 * L)
     assert ref.mul_check(1, A, L, L, A, L, L, dS.numpy(), 2 * L)
+
+
+def _ragged_case(ctx, La, Lb, rng):
+    La, Lb = list(La), list(Lb)
+    offA = np.concatenate([[0], np.cumsum(La)[:-1]]).astype(np.uint64)
+    offB = np.concatenate([[0], np.cumsum(Lb)[:-1]]).astype(np.uint64)
+    Lc = [a + b for a, b in zip(La, Lb)]
+    offC = np.concatenate([[0], np.cumsum(Lc)[:-1]]).astype(np.uint64)
+    A = rng.integers(0, 1 << 32, size=max(1, sum(La)), dtype=np.uint64).astype(np.uint32)
+    B = rng.integers(0, 1 << 32, size=max(1, sum(Lb)), dtype=np.uint64).astype(np.uint32)
+    C = np.full(max(1, sum(Lc)), 0xA5A5A5A5, dtype=np.uint32)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    ctx.mul_ragged(dA.ptr, offA, La, dB.ptr, offB, Lb, dC.ptr, offC)
+    got = dC.numpy()
+    for i in range(len(La)):
+        a = ref.row_int(A[int(offA[i]):], 0, La[i], La[i])
+        b = ref.row_int(B[int(offB[i]):], 0, Lb[i], Lb[i])
+        c = ref.row_int(got[int(offC[i]):], 0, Lc[i], Lc[i])
+        assert c == a * b, (i, La[i], Lb[i])
+
+
+def test_ragged_uneven_pairs(ctx):
+    """One call for pairs of independent, uneven lengths (log-uniform in
+    [1, 4096], a few empty operands, either operand the longer): schoolbook,
+    NTT buckets and zero products mixed."""
+    rng = np.random.default_rng(0xC2)
+    n = 300
+    La = [int(2 ** rng.uniform(0, 12)) for _ in range(n)]
+    Lb = [int(2 ** rng.uniform(0, 12)) for _ in range(n)]
+    La[5], Lb[9] = 0, 0
+    _ragged_case(ctx, La, Lb, rng)
+
+
+def test_ragged_large_and_single(ctx):
+    rng = np.random.default_rng(7)
+    _ragged_case(ctx, [70000, 3, 130000], [50000, 90000, 1], rng)
+    _ragged_case(ctx, [1], [1], rng)
