@@ -122,9 +122,9 @@ __global__ void __launch_bounds__(32 * kWarpProducts) k_school_warp(const uint32
     }
 }
 
-// rows: optional per-product descriptors (ragged batches); null = uniform
-// La, Lb and strides.
-template <int kSchoolThreads>
+// RAGGED: per-product descriptors (rows) give each product's offsets and
+// lengths; otherwise La_u, Lb_u and the strides apply to every row.
+template <int kSchoolThreads, bool RAGGED>
 __global__ void __launch_bounds__(kSchoolThreads) k_school_cols(const uint32_t *__restrict__ A,
                                                                 const uint32_t *__restrict__ B,
                                                                 uint32_t *__restrict__ C, uint32_t N,
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kSchoolThreads) k_school_cols(const uint32_t *
     __shared__ uint32_t sb[kSchoolMaxL + kSchoolMaxL + 8];
     __shared__ uint32_t sg[kSchoolThreads / 32], sp[kSchoolThreads / 32];
     for (uint32_t row = blockIdx.x; row < N; row += gridDim.x) {
-        const RaggedRow d = rows ? rows[row] : RaggedRow{row * sA, row * sB, row * sC, La_u, Lb_u};
+        const RaggedRow d = RAGGED ? rows[row] : RaggedRow{row * sA, row * sB, row * sC, La_u, Lb_u};
         const uint32_t La = d.La, Lb = d.Lb;
         const uint32_t kPad = La + 4;
         const uint32_t Lc = La + Lb;
@@ -238,11 +238,11 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
         // one CTA per product, 4 output columns per thread
         const uint32_t g = grid_for(N, 1, kNumSMs * 16);
         if (La + Lb <= 256u)
-            k_school_cols<64><<<g, 64, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
+            k_school_cols<64, false><<<g, 64, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
         else if (La + Lb <= 512u)
-            k_school_cols<128><<<g, 128, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
+            k_school_cols<128, false><<<g, 128, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
         else
-            k_school_cols<256><<<g, 256, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
+            k_school_cols<256, false><<<g, 256, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC, nullptr);
         count_launch();
     }
 }
@@ -254,7 +254,7 @@ void school_mul_ragged(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32
     if (N == 0u) return;
     cudaStream_t st = current_stream();
     KernelTimed kt("schoolbook", 8.0 * (double)limb_products);
-    k_school_cols<256><<<grid_for(N, 1, kNumSMs * 16), 256, 0, st>>>(A, B, C, N, 0u, 0u, 0u, 0u, 0u, rows);
+    k_school_cols<256, true><<<grid_for(N, 1, kNumSMs * 16), 256, 0, st>>>(A, B, C, N, 0u, 0u, 0u, 0u, 0u, rows);
     count_launch();
 }
 

@@ -296,11 +296,17 @@ __device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a,
     }
 }
 
+template <int LOG_R, bool PAIR>
+constexpr size_t cols_smem_bytes() {   // one or two padded tiles + the twiddle levels
+    return (size_t)(PAIR ? 2 : 1) * kTilePad * 4u + (size_t)((1 << LOG_R) - 1) * 8u;
+}
+
 template <int LOG_R, bool FROM_LIMBS, bool INVERSE, bool PAIR>
 __global__ void __launch_bounds__(kThreads, PAIR ? 3 : 4) k_cols_r(NttParams P, ColsArgs a) {
-    __shared__ uint32_t Sm[PAIR ? 2 * kTilePad : kTilePad];
-    __shared__ uint2 tw[(1 << LOG_R) - 1];
+    extern __shared__ uint4 cols_smem[];
+    uint32_t *Sm = reinterpret_cast<uint32_t *>(cols_smem);
     uint32_t *Sm2 = PAIR ? Sm + kTilePad : Sm;
+    uint2 *tw = reinterpret_cast<uint2 *>(Sm + (PAIR ? 2 : 1) * kTilePad);
     uint64_t b;
     const int q = grid_prime(b);
     if (q == 0)
@@ -655,24 +661,46 @@ static Shape shape_for(uint32_t La, uint32_t Lb) {
 // Paired passes exist for R >= 32 only (shorter columns twist per residue
 // and would spill with two operands).
 constexpr int kPairMinLogR = 5;
+// Column lengths up to 1024 run as one pass (tiles of 4096 / R columns; for
+// R = 1024 a row segment is half a 32-byte sector, whose other half the
+// neighbouring tile reads at the same time from L2).  Longer columns are
+// split in two passes: single passes of 2048 / 4096 points measured slower
+// (K = 2^23: 0.82 against 0.72 ms) with their 4095-entry twiddle tables per
+// CTA and 4- / 8-byte row segments; K = 2^22 runs 0.36 ms in one 1024-point
+// pass against 0.41 ms in two.
+constexpr int kOnePassMaxLog = 10;
+
+template <int LOG_R, bool FL, bool INV, bool PAIR>
+static void cols_launch(unsigned blocks, const NttParams &P, const ColsArgs &a, cudaStream_t st) {
+    constexpr size_t smem = cols_smem_bytes<LOG_R, PAIR>();
+    static bool attr = false;
+    if (!attr) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_cols_r<LOG_R, FL, INV, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        attr = true;
+    }
+    k_cols_r<LOG_R, FL, INV, PAIR><<<blocks, kThreads, smem, st>>>(P, a);
+}
 
 template <bool FL, bool INV, bool PAIR>
 static void cols_r_dispatch(int log_r, unsigned blocks, const NttParams &P, const ColsArgs &a, cudaStream_t st) {
     if constexpr (!PAIR) {
         switch (log_r) {
-            case 1: k_cols_r<1, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
-            case 2: k_cols_r<2, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
-            case 3: k_cols_r<3, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
-            case 4: k_cols_r<4, FL, INV, false><<<blocks, kThreads, 0, st>>>(P, a); return;
+            case 1: cols_launch<1, FL, INV, false>(blocks, P, a, st); return;
+            case 2: cols_launch<2, FL, INV, false>(blocks, P, a, st); return;
+            case 3: cols_launch<3, FL, INV, false>(blocks, P, a, st); return;
+            case 4: cols_launch<4, FL, INV, false>(blocks, P, a, st); return;
             default: break;
         }
     }
     switch (log_r) {
-        case 5: k_cols_r<5, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 6: k_cols_r<6, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 7: k_cols_r<7, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
-        case 8: k_cols_r<8, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
-        default: k_cols_r<9, FL, INV, PAIR><<<blocks, kThreads, 0, st>>>(P, a); break;
+        case 5: cols_launch<5, FL, INV, PAIR>(blocks, P, a, st); break;
+        case 6: cols_launch<6, FL, INV, PAIR>(blocks, P, a, st); break;
+        case 7: cols_launch<7, FL, INV, PAIR>(blocks, P, a, st); break;
+        case 8: cols_launch<8, FL, INV, PAIR>(blocks, P, a, st); break;
+        case 9: cols_launch<9, FL, INV, PAIR>(blocks, P, a, st); break;
+        default: cols_launch<10, FL, INV, PAIR>(blocks, P, a, st); break;
     }
 }
 
@@ -829,7 +857,7 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         const int rest = log_k - log_c;
         int passes[2];
         int npass;
-        if (rest <= 9) {
+        if (rest <= kOnePassMaxLog) {
             passes[0] = rest;
             npass = 1;
         } else {
