@@ -134,12 +134,16 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
                 uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC);
 bool school_thread_fits(uint32_t La, uint32_t Lb);
 
-// Largest L_a + L_b handled by schoolbook.  The reference switches at 1024
-// (batch_arith.cu:181); on B200 this library's NTT overtakes its schoolbook
-// kernels between 384 and 512 limbs (batched products of 2^27 limbs in total:
-// 384 -> 3.8 ms school / 4.7 ms NTT, 512 -> 4.6 / 3.7 ms), so the switch is
-// at 448.  The product is exact either way.  Overridable for tuning with
+// Largest L_a + L_b handled by schoolbook.  The public batch_mp_mul keeps the
+// reference's rule (schoolbook up to 1024, batch_arith.cu:181: such products
+// never grow the context workspace, which gpupi's own tests check).  The
+// library's own algorithms (pi pipeline, decimal conversion, ragged batches)
+// use mul_tuned: on B200 this library's NTT overtakes its schoolbook kernels
+// between 384 and 512 limbs (batched products of 2^27 limbs in total:
+// 384 -> 3.8 ms school / 4.7 ms NTT, 512 -> 4.6 / 3.7 ms), so its switch is at
+// 448.  The product is exact either way.  Overridable for tuning with
 // gpupi_set_mul_crossover().
+constexpr uint32_t kRefSchoolMax = 1024u;
 static uint32_t g_school_max = 448u;
 
 }  // namespace gpupi
@@ -241,7 +245,9 @@ cudaError_t batch_mp_ensure_workspace(BatchMPContext *ctx, size_t required_bytes
     return ensure_workspace(ctx, required_bytes);
 }
 
-cudaError_t batch_mp_mul(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+namespace gpupi {
+static cudaError_t mul_with(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C,
+                            uint32_t school_max) {
     if (!ctx || !valid_array(A) || !valid_array(B) || !valid_array(C)) return cudaErrorInvalidValue;
     if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
     if ((uint64_t)C.length != (uint64_t)A.length + B.length) return cudaErrorInvalidValue;
@@ -249,7 +255,7 @@ cudaError_t batch_mp_mul(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, Ba
     const uint32_t L = A.length + B.length;
     const bool school = A.length == 0u || B.length == 0u ||
                         gpupi::school_thread_fits(A.length, B.length) ||
-                        (L <= gpupi::g_school_max && L <= (uint32_t)BATCH_MUL_NAIVE_L_MAX);
+                        (L <= school_max && L <= (uint32_t)BATCH_MUL_NAIVE_L_MAX);
     if (school) {
         gpupi::school_mul(A.data, B.data, C.data, A.batch_size, A.length, B.length, A.stride, B.stride,
                           C.stride);
@@ -260,6 +266,14 @@ cudaError_t batch_mp_mul(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, Ba
     batch_mul_ntt(A.data, B.data, C.data, ctx->workspace, ctx->ntt_tables, A.batch_size, A.length,
                   B.length, A.stride, B.stride, C.stride);
     return cudaGetLastError();
+}
+cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+    return mul_with(ctx, A, B, C, g_school_max);
+}
+}  // namespace gpupi
+
+cudaError_t batch_mp_mul(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C) {
+    return gpupi::mul_with(ctx, A, B, C, gpupi::kRefSchoolMax);
 }
 
 cudaError_t batch_mp_mul_small(BatchMPContext *ctx, BatchMPArray A, uint32_t B, BatchMPArray C) {

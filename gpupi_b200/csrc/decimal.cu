@@ -26,6 +26,8 @@
 
 namespace gpupi {
 
+cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
+
 constexpr uint32_t kTen9 = 1000000000u;
 
 // out(pos) for the digit of place 10^-k (k = 1..L_dec):
@@ -284,7 +286,7 @@ cudaError_t convert_decimal_precompute_powers(BatchMPContext *ctx, ConvertDecima
     for (uint32_t l = 1; l < levels; ++l) {
         BatchMPArray next = power_array(powers[l - 1].length * 2u);
         if (next.data == nullptr) return fail(l, cudaErrorMemoryAllocation);
-        err = batch_mp_mul(ctx, powers[l - 1], powers[l - 1], next);
+        err = mul_tuned(ctx, powers[l - 1], powers[l - 1], next);
         if (err == cudaSuccess) err = next.compact(ctx);
         if (err != cudaSuccess) {
             power_release(next);
@@ -374,7 +376,7 @@ cudaError_t convert_decimal_equal_split(BatchMPContext *ctx, BatchMPArray input,
             BatchMPArray mA{mant.p, mant_len, rows, mant_len};
             BatchMPArray pB{pw.data, pw.length, rows, 0u};
             BatchMPArray pC{prod.p, mant_len + pw.length, rows, mant_len + pw.length};
-            err = batch_mp_mul(ctx, mA, pB, pC);
+            err = mul_tuned(ctx, mA, pB, pC);
             if (err != cudaSuccess) return err;
             extract_shifted(pC, next, nl, nl, rows, mant_bits - cb, 1u);
             current = BatchMPArray{next, nl, rows * 2u, nl};

@@ -8,7 +8,7 @@
 //     every product's offsets and lengths from a descriptor array;
 //   * otherwise by transform size 2^ceil(log2(L_a + L_b - 1)): each bucket's
 //     operands are gathered into zero-padded rows (longer operand first: the
-//     product commutes), multiplied as one uniform batch (batch_mp_mul), and
+//     product commutes), multiplied as one uniform batch (mul_tuned), and
 //     the L_a + L_b limbs of each row scattered to the product's output.
 //     Zeros above an operand leave the low L_a + L_b limbs of the product
 //     unchanged.
@@ -25,6 +25,7 @@ namespace gpupi {
 void school_mul_ragged(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, const RaggedRow *rows,
                        uint64_t limb_products);
 uint32_t school_max();
+cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 
 namespace {
 
@@ -117,7 +118,7 @@ cudaError_t ntt_bucket(BatchMPContext *ctx, const std::vector<RaggedRow> &rows, 
     }
     if (err == cudaSuccess) {
         const BatchMPArray a{pa, ma, n, ma}, b{pb, mb, n, mb}, c{pc, (uint32_t)lc, n, (uint32_t)lc};
-        err = batch_mp_mul(ctx, a, b, c);
+        err = mul_tuned(ctx, a, b, c);
     }
     if (err == cudaSuccess) {
         k_scatter_rows<<<grid_rows(n), 256, 0, st>>>(C, pc, lc, dr, n);

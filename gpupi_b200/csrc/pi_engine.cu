@@ -137,7 +137,7 @@ static cudaError_t p_mul(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, Batc
                          const char *label, uint32_t n1) {
     return stage(pr, "mul", label, n1, A.batch_size, A.length, B.length,
                  (size_t)A.length + B.length > (size_t)BATCH_MUL_NAIVE_L_MAX,
-                 [&]() { return batch_mp_mul(ctx, A, B, C); });
+                 [&]() { return mul_tuned(ctx, A, B, C); });
 }
 static cudaError_t p_compact(BatchMPContext *ctx, Profiler *pr, BatchMPArray &A, const char *label, uint32_t n1) {
     return stage(pr, "compact", label, n1, A.batch_size, A.length, 0, false, [&]() { return A.compact(ctx); });

@@ -46,6 +46,8 @@ uint32_t round_up_decimal_digits(uint32_t requested, uint32_t *leaf_out);
 uint32_t prec_limbs_for_digits(uint32_t digits);
 
 cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
+// batch_mp_mul with this library's schoolbook/NTT crossover (school_max()).
+cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 void set_school_max(uint32_t v);
 uint32_t school_max();
 
