@@ -283,6 +283,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     g.timer_enable(False)
     ktimes = g.timer_report()
+    kgaps = g.timer_gaps()
     ms_timed_local = e2.elapsed_time(e3) / args.steps
 
     # end to end through the C ABI, digits + RET copied to pinned host memory
@@ -352,6 +353,7 @@ def run_ours(args, ws, rank, local):
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "working set (tens of GB) larger than L2; no flush needed"},
         "pipeline_elapsed_ms": statistics.mean(inner),
+        "step_ms": [round(x, 3) for x in inner],
         "ms_per_step_with_kernel_timers": ms_timed_local,
         "ret_len": r.ret_len, "ret_hash": ret_hash, "convert_digits": r.convert_digits,
         "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": (h1 - h0) // args.steps,
@@ -359,6 +361,11 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": launches,
         "roofline": roof,
         "kernel_families": families,
+        "launch_gaps": {
+            "device_ms_per_step": sum(v[1] for v in kgaps.values()) / args.steps,
+            "top": {k: {"per_step": v[0] / args.steps, "device_ms": v[1] / args.steps,
+                        "host_ms": v[2] / args.steps}
+                    for k, v in sorted(kgaps.items(), key=lambda kv: -kv[1][1])[:8]}},
         "clocks": clk,
         "cpu_baseline": cpu,
         "bbp_check": bbp,

@@ -61,6 +61,8 @@ _SIGS = [
     ("gpupi_timer_reset", ctypes.c_int, []),
     ("gpupi_timer_report", ctypes.c_size_t, [_p, ctypes.c_size_t]),
     ("gpupi_transfer_bytes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    ("gpupi_scratch_stats", ctypes.c_int,
+     [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     ("gpupi_mp_add_noalloc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32, _u32]),
     ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
     ("gpupi_bbp_fractions", ctypes.c_int, [_p, _u32, _p]),
@@ -272,7 +274,24 @@ def timer_report() -> dict:
     out = {}
     for line in buf.value.decode().splitlines():
         name, cnt, ms, by = line.split()
-        out[name] = (int(cnt), float(ms), float(by))
+        if not name.startswith("gap:"):
+            out[name] = (int(cnt), float(ms), float(by))
+    return out
+
+
+def timer_gaps() -> dict:
+    """{"prev>next": (count, device_ms, host_ms)}: time between consecutive
+    timed launches of two kernel families (untimed kernels, synchronisations,
+    launch starvation) on the device and on the host clock."""
+    l = lib()
+    n = l.gpupi_timer_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    l.gpupi_timer_report(buf, n + 1)
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms, host = line.split()
+        if name.startswith("gap:"):
+            out[name[4:]] = (int(cnt), float(ms), float(host))
     return out
 
 
@@ -280,6 +299,13 @@ def transfer_bytes() -> tuple[int, int]:
     h, d = ctypes.c_uint64(0), ctypes.c_uint64(0)
     lib().gpupi_transfer_bytes(ctypes.byref(h), ctypes.byref(d))
     return h.value, d.value
+
+
+def scratch_stats() -> dict:
+    """Scratch arena: {"block_bytes", "high_water", "spills"} (see gpupi_c.h)."""
+    b, h, n = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+    lib().gpupi_scratch_stats(ctypes.byref(b), ctypes.byref(h), ctypes.byref(n))
+    return {"block_bytes": b.value, "high_water": h.value, "spills": n.value}
 
 
 def set_mul_crossover(v: int) -> None:

@@ -23,6 +23,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <new>
@@ -52,7 +53,11 @@ struct TimerRec {
     const char *name;
     cudaEvent_t a, b;
     double bytes;
+    double host_a, host_b;   // host clock (ms) when a and b were recorded
 };
+double host_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 struct TimerState {
     std::mutex mu;
     bool on = false;
@@ -86,7 +91,7 @@ int kernel_timer_begin(const char *name) {
     TimerState &t = timer();
     if (!t.on) return -1;
     std::lock_guard<std::mutex> g(t.mu);
-    TimerRec r{name, pool_event(t), pool_event(t), 0.0};
+    TimerRec r{name, pool_event(t), pool_event(t), 0.0, host_ms(), 0.0};
     cudaEventRecord(r.a, g_stream);
     t.recs.push_back(r);
     return (int)t.recs.size() - 1;
@@ -97,6 +102,7 @@ void kernel_timer_end(int slot, double bytes) {
     std::lock_guard<std::mutex> g(t.mu);
     cudaEventRecord(t.recs[slot].b, g_stream);
     t.recs[slot].bytes = bytes;
+    t.recs[slot].host_b = host_ms();
 }
 size_t kernel_timer_report(char *buf, size_t cap) {
     TimerState &t = timer();
@@ -115,11 +121,33 @@ size_t kernel_timer_report(char *buf, size_t cap) {
         x.ms += ms;
         x.bytes += r.bytes;
     }
+    // Time between consecutive timed launches, keyed by the two families:
+    // untimed kernels, host synchronisations and launch starvation.  The
+    // host figure is the host clock between recording the two events; a
+    // device gap close to it means the device waited for the host.
+    struct Gap {
+        uint64_t n = 0;
+        double ms = 0, host = 0;
+    };
+    std::map<std::string, Gap> gaps;
+    for (size_t i = 1; i < t.recs.size(); ++i) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t.recs[i - 1].b, t.recs[i].a) != cudaSuccess) continue;
+        Gap &x = gaps[std::string(t.recs[i - 1].name) + ">" + t.recs[i].name];
+        x.n++;
+        x.ms += ms;
+        x.host += t.recs[i].host_a - t.recs[i - 1].host_b;
+    }
     std::string out;
     char line[256];
     for (auto &kv : agg) {
         snprintf(line, sizeof(line), "%s %llu %.6f %.0f\n", kv.first.c_str(), (unsigned long long)kv.second.n,
                  kv.second.ms, kv.second.bytes);
+        out += line;
+    }
+    for (auto &kv : gaps) {
+        snprintf(line, sizeof(line), "gap:%s %llu %.6f %.6f\n", kv.first.c_str(), (unsigned long long)kv.second.n,
+                 kv.second.ms, kv.second.host);
         out += line;
     }
     if (buf && cap) {
@@ -229,6 +257,7 @@ BatchMPContext *batch_mp_init() {
         delete ctx;
         return nullptr;
     }
+    gpupi::scratch_context_opened();
     return ctx;
 }
 
@@ -236,6 +265,7 @@ void batch_mp_destroy(BatchMPContext *ctx) {
     if (!ctx) return;
     release_context(ctx);
     delete ctx;
+    gpupi::scratch_context_closed();
 }
 
 size_t batch_mp_workspace_size(const BatchMPContext *ctx) { return ctx ? ctx->workspace_size_bytes : 0u; }

@@ -119,7 +119,7 @@ cudaError_t bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *f
         if (positions[i] > (1ull << 30)) return cudaErrorInvalidValue;   // moduli stay below 2^34
     cudaStream_t st = current_stream();
     unsigned long long *acc = nullptr;
-    cudaError_t err = cudaMallocAsync((void **)&acc, (size_t)count * 8u, st);
+    cudaError_t err = scratch_alloc((void **)&acc, (size_t)count * 8u);
     if (err != cudaSuccess) return err;
     err = cudaMemsetAsync(acc, 0, (size_t)count * 8u, st);
     for (uint32_t i = 0; i < count && err == cudaSuccess; ++i) {
@@ -130,7 +130,7 @@ cudaError_t bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *f
     if (err == cudaSuccess) err = cudaMemcpyAsync(fractions, acc, (size_t)count * 8u, cudaMemcpyDeviceToHost, st);
     note_d2h((size_t)count * 8u);
     if (err == cudaSuccess) err = cudaStreamSynchronize(st);
-    cudaFreeAsync(acc, st);
+    scratch_free(acc);
     return err;
 }
 

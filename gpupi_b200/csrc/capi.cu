@@ -217,6 +217,11 @@ int gpupi_transfer_bytes(uint64_t *h2d, uint64_t *d2h) {
     return 0;
 }
 
+int gpupi_scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills) {
+    gpupi::scratch_stats(block_bytes, high_water, spills);
+    return 0;
+}
+
 int gpupi_set_mul_crossover(uint32_t v) {
     if (v > (uint32_t)BATCH_MUL_NAIVE_L_MAX) return (int)cudaErrorInvalidValue;
     gpupi::set_school_max(v);

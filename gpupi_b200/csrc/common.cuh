@@ -39,6 +39,16 @@ void note_h2d(uint64_t bytes);
 void note_d2h(uint64_t bytes);
 void transfer_bytes(uint64_t *h2d, uint64_t *d2h);
 
+// Device scratch for the library's temporaries: a per-stream arena with no
+// driver call in steady state (scratch.cu).  Freed ranges are reused only by
+// work issued later on the same stream.
+cudaError_t scratch_alloc(void **p, size_t bytes);
+void scratch_free(void *p);
+void scratch_reserve(size_t bytes);   // grow the idle arena of the current stream
+void scratch_context_opened();
+void scratch_context_closed();
+void scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills);
+
 // Optional per-kernel timing: when enabled, the launch sites bracket each
 // launch with CUDA events on the current stream and record the launch's
 // algorithmic HBM bytes.  Resolved (after a synchronisation) by

@@ -225,28 +225,25 @@ static std::vector<uint32_t> pow5(uint32_t e) {
     return v;
 }
 
-// Stream-ordered scratch buffer (no device-wide synchronisation on free).
+// Scratch buffer from the stream's arena (no synchronisation on free).
 struct DevBuf {
     uint32_t *p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFreeAsync(p, current_stream());
-    }
+    ~DevBuf() { scratch_free(p); }
     cudaError_t alloc(size_t words) {
-        if (p) cudaFreeAsync(p, current_stream());
+        scratch_free(p);
         p = nullptr;
-        return words ? cudaMallocAsync((void **)&p, words * 4, current_stream()) : cudaSuccess;
+        return words ? scratch_alloc((void **)&p, words * 4) : cudaSuccess;
     }
 };
 
-// One row of the power table, from the stream-ordered pool.
+// One row of the power table, from the stream's arena.
 BatchMPArray power_array(uint32_t length) {
     BatchMPArray a{nullptr, length, 1u, length};
-    if (length && cudaMallocAsync((void **)&a.data, (size_t)length * 4, current_stream()) != cudaSuccess)
-        a = BatchMPArray{};
+    if (length && scratch_alloc((void **)&a.data, (size_t)length * 4) != cudaSuccess) a = BatchMPArray{};
     return a;
 }
 void power_release(BatchMPArray &a) {
-    if (a.data) cudaFreeAsync(a.data, current_stream());
+    scratch_free(a.data);
     a = BatchMPArray{};
 }
 

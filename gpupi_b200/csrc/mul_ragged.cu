@@ -12,7 +12,7 @@
 //     the L_a + L_b limbs of each row scattered to the product's output.
 //     Zeros above an operand leave the low L_a + L_b limbs of the product
 //     unchanged.
-// Device scratch comes from the stream-ordered pool.
+// Device scratch comes from the stream's scratch arena.
 #include "common.cuh"
 #include "batch_arith.h"
 
@@ -96,10 +96,10 @@ cudaError_t ntt_bucket(BatchMPContext *ctx, const std::vector<RaggedRow> &rows, 
     const uint64_t lc = (uint64_t)ma + mb;
     uint32_t *pa = nullptr, *pb = nullptr, *pc = nullptr;
     RaggedRow *dr = nullptr;
-    cudaError_t err = cudaMallocAsync((void **)&pa, (size_t)n * ma * 4, st);
-    if (err == cudaSuccess) err = cudaMallocAsync((void **)&pb, (size_t)n * mb * 4, st);
-    if (err == cudaSuccess) err = cudaMallocAsync((void **)&pc, (size_t)n * lc * 4, st);
-    if (err == cudaSuccess) err = cudaMallocAsync((void **)&dr, (size_t)n * sizeof(RaggedRow), st);
+    cudaError_t err = scratch_alloc((void **)&pa, (size_t)n * ma * 4);
+    if (err == cudaSuccess) err = scratch_alloc((void **)&pb, (size_t)n * mb * 4);
+    if (err == cudaSuccess) err = scratch_alloc((void **)&pc, (size_t)n * lc * 4);
+    if (err == cudaSuccess) err = scratch_alloc((void **)&dr, (size_t)n * sizeof(RaggedRow));
     if (err == cudaSuccess) {
         err = cudaMemcpyAsync(dr, ord.data(), (size_t)n * sizeof(RaggedRow), cudaMemcpyHostToDevice, st);
         note_h2d((size_t)n * sizeof(RaggedRow));
@@ -125,10 +125,10 @@ cudaError_t ntt_bucket(BatchMPContext *ctx, const std::vector<RaggedRow> &rows, 
         count_launch();
         err = cudaGetLastError();
     }
-    if (pa) cudaFreeAsync(pa, st);
-    if (pb) cudaFreeAsync(pb, st);
-    if (pc) cudaFreeAsync(pc, st);
-    if (dr) cudaFreeAsync(dr, st);
+    scratch_free(pa);
+    scratch_free(pb);
+    scratch_free(pc);
+    scratch_free(dr);
     return err;
 }
 
@@ -161,7 +161,7 @@ cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const
         std::vector<RaggedRow> both(zero);
         both.insert(both.end(), school.begin(), school.end());
         RaggedRow *dr = nullptr;
-        err = cudaMallocAsync((void **)&dr, both.size() * sizeof(RaggedRow), st);
+        err = scratch_alloc((void **)&dr, both.size() * sizeof(RaggedRow));
         if (err == cudaSuccess) {
             err = cudaMemcpyAsync(dr, both.data(), both.size() * sizeof(RaggedRow), cudaMemcpyHostToDevice, st);
             note_h2d(both.size() * sizeof(RaggedRow));
@@ -173,7 +173,7 @@ cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const
         if (err == cudaSuccess && !school.empty())
             school_mul_ragged(A, B, C, (uint32_t)school.size(), dr + zero.size(), school_work);
         if (err == cudaSuccess) err = cudaGetLastError();
-        if (dr) cudaFreeAsync(dr, st);
+        scratch_free(dr);
     }
     for (auto &kv : ntt) {
         if (err != cudaSuccess) break;

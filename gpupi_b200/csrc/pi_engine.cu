@@ -5,8 +5,9 @@
 // with the same operand lengths (including every compact()-derived length),
 // so every intermediate integer, the RET value and the digits are identical.
 // All limb work is done by this library's kernels on the current stream.
-// Temporary device buffers come from the stream-ordered allocator
-// (cudaMallocAsync), so per-level allocation costs no device synchronisation.
+// Temporary device buffers come from the stream's scratch arena (scratch.cu):
+// per-level allocation costs neither a device synchronisation nor, after
+// the first call, any driver call.
 #include "common.cuh"
 #include "batch_arith.h"
 #include "batch_mul_naive.h"
@@ -180,7 +181,7 @@ static cudaError_t p_shift(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, Ba
                  [&]() { return batch_mp_shift_bits(ctx, A, B, s); });
 }
 
-// Stream-ordered device buffer.
+// Device buffer from the stream's scratch arena.
 struct Buf {
     uint32_t *p = nullptr;
     Buf() = default;
@@ -188,13 +189,13 @@ struct Buf {
     Buf &operator=(const Buf &) = delete;
     ~Buf() { reset(); }
     void reset() {
-        if (p) cudaFreeAsync(p, current_stream());
+        scratch_free(p);
         p = nullptr;
     }
     cudaError_t alloc(size_t words) {
         reset();
         if (words == 0) words = 1;
-        return cudaMallocAsync(&p, words * 4, current_stream());
+        return scratch_alloc((void **)&p, words * 4);
     }
     void swap(Buf &o) { std::swap(p, o.p); }
 };
@@ -727,23 +728,23 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
-    // Size the multiply workspace once for the largest product (P * invQ, two
-    // operands of about prec_limbs limbs) so that no level regrows it.
-    {
-        const cudaError_t werr =
-            batch_mp_ensure_workspace(ctx, batch_mul_ntt_workspace_size(1u, prec + 8u, prec + 8u));
-        if (werr != cudaSuccess) {
-            if (own_ctx) batch_mp_destroy(ctx);
-            return werr;
-        }
-    }
     Profiler prof;
     prof.on = req.profile_stages;
     const uint32_t levels = convert ? (uint32_t)__builtin_ctz(convert / leaf) : 0u;
+    // The timed region starts here, before any allocation, as the
+    // reference's does (its workspace and buffers are allocated inside it).
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaError_t err = cudaEventRecord(e0, st);
+    // Size the multiply workspace once for the largest product (P * invQ, two
+    // operands of about prec_limbs limbs) so that no level regrows it, and
+    // the scratch arena for every level's temporaries (at most about 16
+    // bytes per digit at 3e8 and 1e9 digits; the margin absorbs
+    // fragmentation, and a request that still misses spills to the pool).
+    if (err == cudaSuccess)
+        err = batch_mp_ensure_workspace(ctx, batch_mul_ntt_workspace_size(1u, prec + 8u, prec + 8u));
+    if (err == cudaSuccess) scratch_reserve((size_t)requested * 21u + (16u << 20));
     Buf retb;
     BatchMPArray RET{};
     ConvertDecimalPowerTable powers{};
@@ -769,7 +770,7 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
                     leaf, false, [&]() { return convert_decimal_precompute_powers(ctx, &powers, leaf, levels); });
     }
     if (err == cudaSuccess && requested > 0u) {
-        err = cudaMallocAsync((void **)&d_digits, convert, st);
+        err = scratch_alloc((void **)&d_digits, convert);
         if (err == cudaSuccess) {
             BatchMPArray frac = subview(RET, 0u, std::min<uint32_t>(prec, RET.length));
             err = stage(&prof, "decimal_convert", "equal_split", convert, frac.batch_size, frac.length, leaf, false,
@@ -815,7 +816,7 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     }
     if (ret_ready) cudaEventDestroy(ret_ready);
     out.stages = prof.entries;
-    if (d_digits) cudaFreeAsync(d_digits, st);
+    scratch_free(d_digits);
     convert_decimal_release_powers(&powers);
     retb.reset();
     cudaEventDestroy(e0);

@@ -1,0 +1,248 @@
+// Device scratch memory for the library's temporaries (pi pipeline levels,
+// decimal conversion buffers, power tables).
+//
+// One arena per (device, stream): a single device block carved best-fit with
+// coalescing of freed neighbours, all bookkeeping on the host.  A free is
+// immediate on the host; the range is handed out again only to work issued
+// later on the same stream, which the stream runs after every earlier use
+// of it, so no event or synchronisation is needed.
+//
+// A request that does not fit is served by cudaMallocAsync (and released
+// with cudaFreeAsync).  When the arena's live bytes return to zero after
+// such a spill, the block is replaced by one sized from the high-water mark
+// of live bytes, so a repeated workload (the same pi computation again) runs
+// entirely inside the arena after its first call; callers that know their
+// footprint reserve it up front (scratch_reserve).
+//
+// Why not the stream-ordered pool for everything: on B200 (driver 580) a
+// large cudaMallocAsync that maps new memory costs about 6.5 ms of host time
+// per GB, and pool allocations of about 1 GB took 2 to 300 ms each even with
+// the pool told to keep its memory, while the device sat idle.  cudaMalloc
+// maps 21 GB in 3 to 6 ms, so the block comes from cudaMalloc (its free
+// synchronises the device, which only a regrow or the last context's
+// close does).
+//
+// Blocks are released when the last BatchMPContext is destroyed.
+#include "common.cuh"
+
+#include <map>
+#include <mutex>
+#include <unordered_map>
+#include <utility>
+
+namespace gpupi {
+namespace {
+
+constexpr size_t kAlign = 256;
+constexpr size_t kGrain = 2u << 20;
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Arena {
+    cudaStream_t stream = nullptr;
+    char *base = nullptr;
+    size_t cap = 0;
+    std::map<size_t, size_t> free_at;               // offset -> size
+    std::multimap<size_t, size_t> free_by_size;     // size -> offset
+    std::unordered_map<void *, size_t> live;        // arena blocks: ptr -> size
+    std::unordered_map<void *, size_t> spilled;     // cudaMallocAsync blocks: ptr -> size
+    size_t live_bytes = 0, high = 0;
+    uint64_t spills = 0;   // requests ever served outside the block
+    bool grow = false;
+
+    void erase_free(size_t off, size_t size) {
+        free_at.erase(off);
+        auto r = free_by_size.equal_range(size);
+        for (auto it = r.first; it != r.second; ++it)
+            if (it->second == off) {
+                free_by_size.erase(it);
+                return;
+            }
+    }
+    void insert_free(size_t off, size_t size) {
+        auto next = free_at.lower_bound(off);
+        if (next != free_at.end() && off + size == next->first) {
+            const size_t noff = next->first, nsize = next->second;
+            erase_free(noff, nsize);
+            size += nsize;
+        }
+        auto it = free_at.lower_bound(off);
+        if (it != free_at.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == off) {
+                const size_t poff = prev->first, psize = prev->second;
+                erase_free(poff, psize);
+                off = poff;
+                size += psize;
+            }
+        }
+        free_at[off] = size;
+        free_by_size.emplace(size, off);
+    }
+    void reset_block(char *p, size_t bytes) {
+        base = p;
+        cap = bytes;
+        free_at.clear();
+        free_by_size.clear();
+        if (p) insert_free(0, bytes);
+    }
+
+    cudaError_t alloc(void **out, size_t bytes) {
+        const size_t need = round_up(bytes ? bytes : 1, kAlign);
+        auto it = free_by_size.lower_bound(need);
+        if (it != free_by_size.end()) {
+            const size_t size = it->first, off = it->second;
+            erase_free(off, size);
+            if (size > need) insert_free(off + need, size - need);
+            void *p = base + off;
+            live.emplace(p, need);
+            live_bytes += need;
+            high = std::max(high, live_bytes);
+            *out = p;
+            return cudaSuccess;
+        }
+        void *p = nullptr;
+        const cudaError_t err = cudaMallocAsync(&p, need, stream);
+        if (err != cudaSuccess) return err;
+        spilled.emplace(p, need);
+        ++spills;
+        live_bytes += need;
+        high = std::max(high, live_bytes);
+        grow = true;
+        *out = p;
+        return cudaSuccess;
+    }
+
+    // false when p is not one of this arena's blocks
+    bool release(void *p) {
+        auto a = live.find(p);
+        if (a != live.end()) {
+            insert_free((size_t)((char *)p - base), a->second);
+            live_bytes -= a->second;
+            live.erase(a);
+        } else {
+            auto s = spilled.find(p);
+            if (s == spilled.end()) return false;
+            cudaFreeAsync(p, stream);
+            live_bytes -= s->second;
+            spilled.erase(s);
+        }
+        if (live_bytes == 0u && grow) regrow();
+        return true;
+    }
+
+    // Everything is free: replace the block by one with room for the
+    // high-water mark plus a quarter for fragmentation (and never smaller
+    // than one and a half times the old block, so repeated spills converge).
+    void regrow() {
+        grow = false;
+        replace_block(round_up(std::max(high + high / 4, cap + cap / 2), kGrain));
+    }
+
+    // Only while nothing is live.  cudaFree waits for queued work that may
+    // still use the old block.
+    void replace_block(size_t bytes) {
+        if (base) cudaFree(base);
+        reset_block(nullptr, 0);
+        char *p = nullptr;
+        if (cudaMalloc((void **)&p, bytes) != cudaSuccess) {
+            cudaGetLastError();   // keep serving requests by spilling
+            return;
+        }
+        reset_block(p, bytes);
+    }
+
+    // after a device synchronisation (the stream itself may be gone)
+    void drop() {
+        for (auto &kv : spilled) cudaFree(kv.first);
+        spilled.clear();
+        if (base) cudaFree(base);
+        live.clear();
+        reset_block(nullptr, 0);
+        live_bytes = high = 0;
+        grow = false;
+    }
+};
+
+struct Registry {
+    std::mutex mu;
+    std::map<std::pair<int, cudaStream_t>, Arena> arenas;
+    int contexts = 0;
+};
+Registry &registry() {
+    static Registry r;
+    return r;
+}
+
+}  // namespace
+
+cudaError_t scratch_alloc(void **p, size_t bytes) {
+    if (!p) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    const cudaStream_t st = current_stream();
+    Arena &a = r.arenas[{dev, st}];
+    a.stream = st;
+    return a.alloc(p, bytes);
+}
+
+void scratch_free(void *p) {
+    if (!p) return;
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    for (auto &kv : r.arenas)
+        if (kv.second.release(p)) return;
+}
+
+void scratch_reserve(size_t bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    const cudaStream_t st = current_stream();
+    Arena &a = r.arenas[{dev, st}];
+    a.stream = st;
+    if (a.live_bytes != 0u || a.cap >= bytes) return;
+    a.replace_block(round_up(bytes, kGrain));
+}
+
+void scratch_context_opened() {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    ++r.contexts;
+}
+
+void scratch_context_closed() {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    if (r.contexts > 0) --r.contexts;
+    if (r.contexts != 0) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto &kv : r.arenas) {
+        if (kv.first.first != cur) cudaSetDevice(kv.first.first);
+        cudaDeviceSynchronize();
+        kv.second.drop();
+    }
+    cudaSetDevice(cur);
+    r.arenas.clear();
+}
+
+void scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills) {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    uint64_t b = 0, h = 0, s = 0;
+    for (auto &kv : r.arenas) {
+        b += kv.second.cap;
+        h = std::max<uint64_t>(h, kv.second.high);
+        s += kv.second.spills;
+    }
+    if (block_bytes) *block_bytes = b;
+    if (high_water) *high_water = h;
+    if (spills) *spills = s;
+}
+
+}  // namespace gpupi

@@ -113,13 +113,24 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
 
 /* Per-kernel timing: CUDA events around each launch on the current stream,
  * with the launch's algorithmic HBM bytes.  The report has one line per
- * kernel family: "name launches total_ms total_bytes". */
+ * kernel family: "name launches total_ms total_bytes", then one line per
+ * pair of consecutive families: "gap:prev>next count device_ms host_ms",
+ * the device time between the end of one timed launch and the start of
+ * the next, and the host time between recording the two. */
 int gpupi_timer_enable(int on);
 int gpupi_timer_reset(void);
 size_t gpupi_timer_report(char *buf, size_t cap);
 
 /* Cumulative host->device and device->host bytes copied by the library. */
 int gpupi_transfer_bytes(uint64_t *h2d, uint64_t *d2h);
+
+/* Scratch arena used for the library's temporaries (pipeline levels,
+ * conversion buffers): device bytes held in arena blocks, the high-water mark
+ * of live scratch bytes, and how many requests were ever served outside the
+ * blocks (each such spill regrows the arena once its live bytes return to
+ * zero; a repeated workload then adds none).  No counterpart in the
+ * reference, which allocates per call. */
+int gpupi_scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills);
 
 /* Allocation-free batched addition: C = A + B exactly like gpupi_mp_add, but
  * without a context and without allocating.  It has no counterpart in the

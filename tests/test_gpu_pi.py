@@ -66,3 +66,20 @@ def test_pi_1e7_matches_cpp_restatement(ctx):
     assert f"RET_len={r.ret_len}" in out[0]
     assert out[1] == pi_ref.hex_preview("RET", r.ret)
     assert out[3] == f"DEC_hash = {pi_ref.decimal_hash(r.dec)}"
+
+
+def test_scratch_arena_reaches_steady_state(ctx):
+    """Repeating one computation settles the scratch arena: after the first
+    calls the temporaries fit its block (no request served outside it), and
+    every repeat gives the same RET and digits."""
+    import gpupi_b200 as g
+    d = 300_000
+    first = g.pi_compute(d, ctx)
+    g.pi_compute(d, ctx)
+    s0 = g.scratch_stats()
+    r = g.pi_compute(d, ctx)
+    s1 = g.scratch_stats()
+    assert s1["spills"] == s0["spills"]
+    assert s1["block_bytes"] > 0 and s1["high_water"] > 0
+    assert np.array_equal(r.ret, first.ret)
+    assert r.dec == first.dec
