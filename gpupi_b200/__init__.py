@@ -67,6 +67,7 @@ _SIGS = [
     ("gpupi_set_mul_crossover", ctypes.c_int, [_u32]),
     ("gpupi_bbp_fractions", ctypes.c_int, [_p, _u32, _p]),
     ("gpupi_mp_mul_ragged", ctypes.c_int, [_p, _u32, _p, _p, _p, _p, _p, _p, _p, _p]),
+    ("gpupi_mp_mul_spectra", ctypes.c_int, [_p, _u32, _p, _u32, _p, _u32, _p, _u32, _p, _u32, _p, _u32]),
 ]
 
 C_ABI_SYMBOLS = [s[0] for s in _SIGS]
@@ -218,6 +219,11 @@ class Context:
         _check(lib().gpupi_mp_limblength_max(self.h, N, A, La, sA, ctypes.byref(r)), "batch_mp_limblength_max")
         return r.value
 
+    def mul_spectra(self, N, A, La, B, Lb, C, Lc, D=None, Ld=0, E=None, Le=0):
+        """C = A B (+ D E) through shared-transform spectra; packed rows,
+        device pointers (gpupi_mp_mul_spectra)."""
+        _check(lib().gpupi_mp_mul_spectra(self.h, N, A, La, B, Lb, D, Ld, E, Le, C, Lc), "gpupi_mp_mul_spectra")
+
     def mul_ragged(self, A, offA, La, B, offB, Lb, C, offC):
         """Ragged batch: product i = A[offA[i]:+La[i]] * B[offB[i]:+Lb[i]] into
         C[offC[i]:+La[i]+Lb[i]] (device pointers A, B, C; host sequences for the
@@ -334,14 +340,16 @@ def ret_limbs_bound(digits: int) -> int:
 
 def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None = None,
                ret_capacity: int | None = None, device_only: bool = False, profile: bool = False,
-               host_digits=None, host_ret=None) -> PiResult:
+               host_digits=None, host_ret=None, tuned: bool = False) -> PiResult:
     """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional).
 
     ``host_digits`` / ``host_ret``: optional writable host buffers (e.g. pinned
     torch tensors: uint8 for the digits, 32-bit for RET, at least
     ret_limbs_bound(digits) limbs) receiving the digits and RET directly from
     the device.  ``device_only`` keeps RET and the digits on the device (no
-    host copies at all)."""
+    host copies at all).  ``tuned`` shares forward transforms within each
+    merge level of the splitting tree instead of the reference's op sequence
+    (one batched product per op); both give the same RET and digits."""
     _torch()
     l = lib()
     if copy_digits is None:
@@ -360,7 +368,7 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
         dbuf = ctypes.create_string_buffer(max(copy_digits, 1))
         dptr = ctypes.addressof(dbuf) if copy_digits else None
     info = (_u32 * 8)()
-    flags = (1 if profile else 0) | (2 if device_only else 0)
+    flags = (1 if profile else 0) | (2 if device_only else 0) | (4 if tuned else 0)
     rc = l.gpupi_pi_compute(ctx.h if ctx else None, digits, flags, ret.ctypes.data if ret_capacity else None,
                             ret_capacity, dptr, copy_digits, info)
     _check(rc, "gpupi_pi_compute")

@@ -431,6 +431,7 @@ cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, 
                   A.stride, B.stride, C.stride);
     return cudaGetLastError();
 }
+const NTTPrecomputedTables &context_tables(const BatchMPContext *ctx) { return ctx->ntt_tables; }
 void set_school_max(uint32_t v) { g_school_max = v; }
 uint32_t school_max() { return g_school_max; }
 }  // namespace gpupi

@@ -8,8 +8,11 @@
 #include "convert_decimal.h"
 #include "gpupi_c.h"
 #include "pi_engine.h"
+#include "spectrum.h"
 
 #include <string.h>
+
+#include <algorithm>
 
 struct gpupi_ctx {
     BatchMPContext *ctx;
@@ -64,6 +67,36 @@ int gpupi_ctx_ensure_workspace(gpupi_ctx *ctx, size_t bytes) {
 int gpupi_mp_mul(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,
                  uint32_t Lb, uint32_t sB, uint32_t *C, uint32_t Lc, uint32_t sC) {
     return (int)batch_mp_mul(raw(ctx), view(A, La, N, sA), view(B, Lb, N, sB), view(C, Lc, N, sC));
+}
+
+int gpupi_mp_mul_spectra(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, const uint32_t *B,
+                         uint32_t Lb, const uint32_t *D, uint32_t Ld, const uint32_t *E, uint32_t Le, uint32_t *C,
+                         uint32_t Lc) {
+    BatchMPContext *c = raw(ctx);
+    if (!c || !A || !B || !C || N == 0u || La == 0u || Lb == 0u) return (int)cudaErrorInvalidValue;
+    const bool two = D != nullptr;
+    if (two && (!E || Ld == 0u || Le == 0u)) return (int)cudaErrorInvalidValue;
+    const uint64_t need = std::max<uint64_t>((uint64_t)La + Lb, two ? (uint64_t)Ld + Le + 1u : 0u);
+    if (Lc < need) return (int)cudaErrorInvalidValue;
+    const gpupi::SpectrumShape S = gpupi::spectrum_shape(Lc - 1u);
+    const uint32_t las[2] = {La, Ld}, lbs[2] = {Lb, Le};
+    if (S.M == 0 || !gpupi::spectrum_sum_fits(las, lbs, two ? 2 : 1)) return (int)cudaErrorInvalidValue;
+    const uint64_t words = gpupi::spectrum_words(S, N);
+    uint32_t *F[4] = {nullptr, nullptr, nullptr, nullptr}, *flags = nullptr;
+    cudaError_t err = cudaSuccess;
+    for (int i = 0; i < (two ? 4 : 2) && err == cudaSuccess; ++i) err = gpupi::scratch_alloc((void **)&F[i], words * 4);
+    if (err == cudaSuccess) err = gpupi::scratch_alloc((void **)&flags, gpupi::spectrum_flag_words(N, Lc) * 4);
+    if (err == cudaSuccess) {
+        const NTTPrecomputedTables &t = gpupi::context_tables(c);
+        gpupi::spectrum_forward(t, S, N, A, La, La, F[0], B, Lb, Lb, F[1]);
+        if (two) gpupi::spectrum_forward(t, S, N, D, Ld, Ld, F[2], E, Le, Le, F[3]);
+        const uint32_t *X[2] = {F[0], F[2]}, *Y[2] = {F[1], F[3]};
+        gpupi::spectrum_inverse(t, S, N, two ? 2 : 1, X, Y, F[0], C, Lc, Lc, flags);
+        err = cudaGetLastError();
+    }
+    for (int i = 0; i < 4; ++i) gpupi::scratch_free(F[i]);
+    gpupi::scratch_free(flags);
+    return (int)err;
 }
 
 int gpupi_mp_add(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B,
@@ -175,6 +208,7 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
     req.copy_digits = h_digits ? (uint32_t)std::min<size_t>(digits_cap, digits) : 0u;
     req.ctx = raw(ctx);
     req.device_only = (flags & 2u) != 0u;
+    req.tuned = (flags & 4u) != 0u;
     req.host_digits = h_digits;
     req.host_ret = h_ret;
     req.host_ret_cap = h_ret ? ret_cap : 0;

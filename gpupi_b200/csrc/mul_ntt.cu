@@ -32,6 +32,7 @@
 #include "ntt_core.cuh"
 #include "carry_tile.cuh"
 #include "batch_mul_ntt.h"
+#include "spectrum.h"
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -464,6 +465,136 @@ __global__ void __launch_bounds__(128) k_rows_small(NttParams P, RowsArgs a) {
         rows_small_body<2>(P, a, row, SA, SB, twf, twi);
 }
 
+// ---------------------------------------------------------------------------
+// Split row passes for products that share forward transforms.
+//
+// k_rows_fwd finishes the forward transform of one or two operands whose
+// column passes are done and stores each row segment in the thread order of
+// its last stage (thread t holds positions 16t .. 16t + 15: four 16-byte
+// stores).  k_rows_inv reads T pairs of such spectra in the same order,
+// forms sum_t X_t Y_t K^-1 (mod p) and runs the inverse stages, leaving the
+// segment in the order the inverse column passes expect, exactly as the
+// fused k_rows_r does.  So a transform computed once serves every product
+// it takes part in, and a sum of products costs one inverse transform.
+// ---------------------------------------------------------------------------
+constexpr int kSplitLogC = 12;
+using SplitLast = ExecStage<kSplitLogC, 0, false, StagePlan<kSplitLogC>::n - 1>::S;
+static_assert(SplitLast::kLO == 0 && SplitLast::kB == 4, "last row stage holds 16 consecutive positions");
+
+struct RowsFwdArgs {
+    uint32_t *F0;   // spectra [vrow][q][K], column passes done
+    uint32_t *F1;   // second operand of the same shape, or null
+    int log_k;
+};
+
+template <int Q>
+__device__ __forceinline__ void rows_fwd_body(const RowsFwdArgs &a, uint64_t b, uint32_t *Sm, uint2 *tw) {
+    constexpr int C = 1 << kSplitLogC;
+    constexpr int T = C / 16;
+    using First = typename ExecStage<kSplitLogC, 0, false, 0>::S;
+    const uint32_t nseg = 1u << (a.log_k - kSplitLogC);
+    const uint64_t K = 1ull << a.log_k;
+    const uint64_t off = (b / nseg) * 3 * K + (uint64_t)Q * K + ((uint64_t)(b % nseg) << kSplitLogC);
+    const uint32_t t = threadIdx.x;
+    for (int op = 0; op < (a.F1 ? 2 : 1); ++op) {
+        uint32_t *F = (op == 0 ? a.F0 : a.F1) + off;
+        uint32_t x[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            x[j] = F[pos];
+        }
+        __syncthreads();   // twiddles loaded; the previous operand's last stage has left the tile
+        run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
+        uint4 *out = reinterpret_cast<uint4 *>(F + 16u * t);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) out[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
+    }
+    (void)T;
+}
+
+__global__ void __launch_bounds__((1 << kSplitLogC) / 16, 4) k_rows_fwd(NttParams P, RowsFwdArgs a) {
+    extern __shared__ uint4 rows_smem[];
+    constexpr int C = 1 << kSplitLogC;
+    uint32_t *Sm = reinterpret_cast<uint32_t *>(rows_smem);
+    uint2 *tw = reinterpret_cast<uint2 *>(Sm + C + C / 32);
+    uint64_t b;
+    const int q = grid_prime(b);
+    const uint2 *lev = level_ptr(P.tab, 0, q);
+    for (uint32_t e = threadIdx.x; e < C - 1; e += C / 16) tw[e] = __ldg(lev + e);
+    if (q == 0)
+        rows_fwd_body<0>(a, b, Sm, tw);
+    else if (q == 1)
+        rows_fwd_body<1>(a, b, Sm, tw);
+    else
+        rows_fwd_body<2>(a, b, Sm, tw);
+}
+
+constexpr int kMaxTerms = 2;
+struct RowsInvArgs {
+    const uint32_t *X[kMaxTerms];
+    const uint32_t *Y[kMaxTerms];
+    uint32_t *Fout;   // may be one of the X or Y (each CTA reads its segment before writing it)
+    int terms;
+    int log_k;
+};
+
+template <int TERMS, int Q>
+__device__ __forceinline__ void rows_inv_body(const NttParams &P, const RowsInvArgs &a, uint64_t b, uint32_t *Sm,
+                                              uint2 *tw) {
+    using Out = typename ExecStage<kSplitLogC, 0, true, StagePlan<kSplitLogC>::n - 1>::S;
+    const uint32_t nseg = 1u << (a.log_k - kSplitLogC);
+    const uint64_t K = 1ull << a.log_k;
+    const uint64_t off = (b / nseg) * 3 * K + (uint64_t)Q * K + ((uint64_t)(b % nseg) << kSplitLogC);
+    const uint32_t t = threadIdx.x;
+    const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + Q);
+    uint32_t x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = 0u;
+#pragma unroll
+    for (int term = 0; term < TERMS; ++term) {
+        const uint4 *X = reinterpret_cast<const uint4 *>(a.X[term] + off + 16u * t);
+        const uint4 *Y = reinterpret_cast<const uint4 *>(a.Y[term] + off + 16u * t);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const uint4 u = X[v], w = Y[v];
+            x[4 * v] = add_n<Q>(x[4 * v], norm<Q>(mont<Q>(u.x, w.x)));
+            x[4 * v + 1] = add_n<Q>(x[4 * v + 1], norm<Q>(mont<Q>(u.y, w.y)));
+            x[4 * v + 2] = add_n<Q>(x[4 * v + 2], norm<Q>(mont<Q>(u.z, w.z)));
+            x[4 * v + 3] = add_n<Q>(x[4 * v + 3], norm<Q>(mont<Q>(u.w, w.w)));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(x[j], scale));   // sum K^-1
+    __syncthreads();   // inverse twiddles loaded
+    run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        uint32_t pos, c;
+        Out::elem(t, j, pos, c);
+        a.Fout[off + pos] = x[j];
+    }
+}
+
+template <int TERMS>
+__global__ void __launch_bounds__((1 << kSplitLogC) / 16, 4) k_rows_inv(NttParams P, RowsInvArgs a) {
+    extern __shared__ uint4 rows_smem[];
+    constexpr int C = 1 << kSplitLogC;
+    uint32_t *Sm = reinterpret_cast<uint32_t *>(rows_smem);
+    uint2 *tw = reinterpret_cast<uint2 *>(Sm + C + C / 32);
+    uint64_t b;
+    const int q = grid_prime(b);
+    const uint2 *lev = level_ptr(P.tab, 1, q);
+    for (uint32_t e = threadIdx.x; e < C - 1; e += C / 16) tw[e] = __ldg(lev + e);
+    if (q == 0)
+        rows_inv_body<TERMS, 0>(P, a, b, Sm, tw);
+    else if (q == 1)
+        rows_inv_body<TERMS, 1>(P, a, b, Sm, tw);
+    else
+        rows_inv_body<TERMS, 2>(P, a, b, Sm, tw);
+}
+
 // Coset recombination.  Row r holds z_i[j] = C_i[j] g^(ij) for cosets i < M;
 // C_i[j] = sum_b C_b[j] c_i^b, so C_b[j] = sum_i Vinv[b][i] C_i[j].  The M
 // outputs of position j overwrite the M inputs of position j.
@@ -795,6 +926,19 @@ static void coset_matrix(int M, int log_k, uint32_t (&out)[kPrimes][kMaxCosets][
     }
 }
 
+// Column passes below the 4096-point rows: one for up to 2^10 points,
+// else two; returns their count.
+static int column_passes(int log_k, int (&passes)[2]) {
+    const int rest = log_k - 12;
+    if (rest <= kOnePassMaxLog) {
+        passes[0] = rest;
+        return 1;
+    }
+    passes[0] = (rest + 1) / 2;
+    passes[1] = rest / 2;
+    return 2;
+}
+
 static void launch_combine(int M, const NttParams &P, const CombineArgs &c, uint32_t N, cudaStream_t st) {
     const uint64_t K = 1ull << c.log_k;
     const unsigned blocks = (unsigned)((uint64_t)N * kPrimes * (K / kThreads));
@@ -854,17 +998,8 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         count_launch();
     } else {
         const int log_c = 12;
-        const int rest = log_k - log_c;
         int passes[2];
-        int npass;
-        if (rest <= kOnePassMaxLog) {
-            passes[0] = rest;
-            npass = 1;
-        } else {
-            passes[0] = (rest + 1) / 2;
-            passes[1] = rest / 2;
-            npass = 2;
-        }
+        const int npass = column_passes(log_k, passes);
         // forward column passes: A and B together (one launch per pass) unless
         // B is A or a broadcast row
         const bool pair = !square && !bcast && passes[0] >= kPairMinLogR && (npass == 1 || passes[1] >= kPairMinLogR);
@@ -906,6 +1041,100 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         }
     }
     CrtArgs c{FA, log_k, M, C, sC, Lc, (uint32_t)tiles, flags};
+    KernelTimed kt("ntt_crt_carry", 12.0 * (double)Lc * N + 4.0 * (double)Lc * N);
+    k_crt<<<(unsigned)(N * tiles), kThreads, 0, st>>>(c);
+    count_launch();
+    if (tiles > 1) launch_carry_fixup(false, C, sC, N, Lc, (uint32_t)tiles, kCrtSpan, flags, st);
+}
+
+// ---------------------------------------------------------------------------
+// Shared-transform products: spectrum_forward computes the forward transform
+// of one operand (or two of the same shape) into caller buffers;
+// spectrum_inverse turns a sum of products of such spectra into limbs.
+// ---------------------------------------------------------------------------
+static void rows_split_attr() {
+    static bool done = false;
+    if (!done) {
+        constexpr int smem = (int)rows_smem_bytes<kSplitLogC>();
+        cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_rows_inv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_rows_inv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        done = true;
+    }
+}
+
+static void spectrum_forward(const NttParams &P, Shape s, uint32_t N, const uint32_t *X, uint64_t sX, uint32_t Lx,
+                             uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly, uint32_t *FY,
+                             cudaStream_t st) {
+    const int log_k = s.log_k, M = s.M;
+    const uint64_t K = 1ull << log_k;
+    const uint64_t VR = (uint64_t)N * M;
+    int passes[2];
+    const int npass = column_passes(log_k, passes);
+    const bool pair = Y && passes[0] >= kPairMinLogR && (npass == 1 || passes[1] >= kPairMinLogR);
+    for (int op = 0; op < ((pair || !Y) ? 1 : 2); ++op) {
+        const uint32_t *Z = op == 0 ? X : Y;
+        const uint64_t sZ = op == 0 ? sX : sY;
+        const uint32_t Lz = op == 0 ? Lx : Ly;
+        uint32_t *F = op == 0 ? FX : FY;
+        const uint32_t nb = (uint32_t)((Lz + K - 1) / K);
+        const uint32_t nb2 = (uint32_t)((Ly + K - 1) / K);
+        int log_s = log_k;
+        for (int ps = 0; ps < npass; ++ps) {
+            ColsArgs a{Z, sZ, Lz, nb, F, log_k, log_s, M, pair ? Y : nullptr, sY, Ly, nb2, pair ? FY : nullptr};
+            launch_cols_r(ps == 0, false, pair, passes[ps], P, a, VR, st);
+            log_s -= passes[ps];
+        }
+    }
+    rows_split_attr();
+    RowsFwdArgs r{FX, Y ? FY : nullptr, log_k};
+    const unsigned blocks = (unsigned)(VR * kPrimes * (K >> kSplitLogC));
+    KernelTimed kt("ntt_rows_fwd", 8.0 * (double)K * (double)VR * (Y ? 2.0 : 1.0) * kPrimes);
+    k_rows_fwd<<<blocks, (1 << kSplitLogC) / 16, rows_smem_bytes<kSplitLogC>(), st>>>(P, r);
+    count_launch();
+}
+
+static void spectrum_inverse(const NttParams &P, Shape s, uint32_t N, int terms, const uint32_t *const *X,
+                             const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC, uint32_t Lc,
+                             uint32_t *flags, cudaStream_t st) {
+    const int log_k = s.log_k, M = s.M;
+    const uint64_t K = 1ull << log_k;
+    const uint64_t VR = (uint64_t)N * M;
+    rows_split_attr();
+    RowsInvArgs r{};
+    for (int i = 0; i < terms; ++i) {
+        r.X[i] = X[i];
+        r.Y[i] = Y[i];
+    }
+    r.Fout = Fout;
+    r.terms = terms;
+    r.log_k = log_k;
+    const unsigned blocks = (unsigned)(VR * kPrimes * (K >> kSplitLogC));
+    {
+        KernelTimed kt("ntt_rows_inv", 4.0 * (double)K * (double)VR * kPrimes * (2.0 * terms + 1.0));
+        if (terms == 1)
+            k_rows_inv<1><<<blocks, (1 << kSplitLogC) / 16, rows_smem_bytes<kSplitLogC>(), st>>>(P, r);
+        else
+            k_rows_inv<2><<<blocks, (1 << kSplitLogC) / 16, rows_smem_bytes<kSplitLogC>(), st>>>(P, r);
+        count_launch();
+    }
+    int passes[2];
+    const int npass = column_passes(log_k, passes);
+    int log_s = kSplitLogC;
+    for (int ps = npass - 1; ps >= 0; --ps) {
+        log_s += passes[ps];
+        ColsArgs a{nullptr, 0, 0, 0, Fout, log_k, log_s, M, nullptr, 0, 0, 0, nullptr};
+        launch_cols_r(false, true, false, passes[ps], P, a, VR, st);
+    }
+    if (M > 1) {
+        CombineArgs c{};
+        c.F = Fout;
+        c.log_k = log_k;
+        coset_matrix(M, log_k, c.vinv);
+        launch_combine(M, P, c, N, st);
+    }
+    const uint64_t tiles = ((uint64_t)Lc + kCrtSpan - 1) / kCrtSpan;
+    CrtArgs c{Fout, log_k, M, C, sC, Lc, (uint32_t)tiles, flags};
     KernelTimed kt("ntt_crt_carry", 12.0 * (double)Lc * N + 4.0 * (double)Lc * N);
     k_crt<<<(unsigned)(N * tiles), kThreads, 0, st>>>(c);
     count_launch();
@@ -990,3 +1219,47 @@ void batch_mul_ntt(uint32_t *A, uint32_t *B, uint32_t *ret, uint32_t *workspace,
 size_t batch_mul_ntt_workspace_size(uint32_t N, uint32_t L_a, uint32_t L_b) {
     return gpupi::ntt::workspace_bytes(N, L_a, L_b);
 }
+
+namespace gpupi {
+
+SpectrumShape spectrum_shape(uint64_t ncoef) {
+    if (ncoef < 2u || ncoef > ((uint64_t)ntt::kMaxCosets << ntt::kMaxLog)) return SpectrumShape{0, 0};
+    const ntt::Shape s = ntt::shape_for((uint32_t)ncoef, 1u);
+    if (s.log_k <= ntt::kSplitLogC) return SpectrumShape{0, 0};
+    return SpectrumShape{s.log_k, s.M};
+}
+
+uint64_t spectrum_words(SpectrumShape s, uint32_t N) { return (uint64_t)N * s.M * ntt::kPrimes << s.log_k; }
+
+uint64_t spectrum_flag_words(uint32_t N, uint32_t Lc) {
+    return (uint64_t)N * (((uint64_t)Lc + ntt::kCrtSpan - 1) / ntt::kCrtSpan);
+}
+
+bool spectrum_sum_fits(const uint32_t *La, const uint32_t *Lb, int terms) {
+    // every coefficient of sum_t A_t B_t is below sum_t min(La_t, Lb_t) (2^32 - 1)^2,
+    // which must stay below p0 p1 p2 for the CRT to be exact
+    unsigned __int128 bound = 0;
+    for (int t = 0; t < terms; ++t) {
+        const uint64_t m = La[t] < Lb[t] ? La[t] : Lb[t];
+        bound += (unsigned __int128)m * 0xffffffffull * 0xffffffffull;
+    }
+    unsigned __int128 cap = 1;
+    for (int q = 0; q < ntt::kPrimes; ++q) cap *= ntt::kP[q];
+    return bound < cap;
+}
+
+void spectrum_forward(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, const uint32_t *X,
+                      uint64_t sX, uint32_t Lx, uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly,
+                      uint32_t *FY) {
+    const ntt::NttParams P = ntt::make_params(tables);
+    ntt::spectrum_forward(P, ntt::Shape{s.log_k, s.M}, N, X, sX, Lx, FX, Y, sY, Ly, FY, current_stream());
+}
+
+void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, int terms,
+                      const uint32_t *const *X, const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC,
+                      uint32_t Lc, uint32_t *flags) {
+    const ntt::NttParams P = ntt::make_params(tables);
+    ntt::spectrum_inverse(P, ntt::Shape{s.log_k, s.M}, N, terms, X, Y, Fout, C, sC, Lc, flags, current_stream());
+}
+
+}  // namespace gpupi

@@ -14,6 +14,7 @@
 #include "batch_mul_ntt.h"
 #include "convert_decimal.h"
 #include "pi_engine.h"
+#include "spectrum.h"
 
 #include <math.h>
 #include <stdio.h>
@@ -203,12 +204,163 @@ struct Buf {
 static const uint32_t kDivLo = 830297u;       // pi_bs_gpu.cu:147
 static const uint32_t kDivHi = 156590819u;    // pi_bs_gpu.cu:148
 
+// One merge level as the reference issues it (pi_bs_gpu.cu:625-723): four
+// products, the shifted addition or subtraction, three compactions.
+static cudaError_t plain_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, uint32_t n1, uint32_t half,
+                               uint32_t ignore, bool subtract, const BatchMPArray &P, const BatchMPArray &Q,
+                               const BatchMPArray &R, Buf &pn, BatchMPArray &Pn, Buf &qn, BatchMPArray &Qn, Buf &rn,
+                               BatchMPArray &Rn) {
+    Buf r1b, r2b;
+    BatchMPArray P_even{P.data, P.length, half - ignore, P.stride * 2};
+    BatchMPArray P_odd{P.data + P.stride, P.length, half - ignore, P.stride * 2};
+    Pn = BatchMPArray{nullptr, P.length * 2u, half - ignore, P.length * 2u};
+    if (P_odd.batch_size > 0u) {
+        TRY(pn.alloc((size_t)Pn.batch_size * Pn.stride));
+        Pn.data = pn.p;
+        TRY(p_mul(ctx, pr, P_even, P_odd, Pn, "P", n1));
+        TRY(p_compact(ctx, pr, Pn, "P", n1));
+    } else {
+        pn.reset();
+        Pn = BatchMPArray{nullptr, 0, 0, 0};
+    }
+    BatchMPArray Q_even{Q.data, Q.length, half, Q.stride * 2};
+    BatchMPArray Q_odd{Q.data + Q.stride, Q.length, half, Q.stride * 2};
+    Qn = BatchMPArray{nullptr, Q.length * 2u, half, Q.length * 2u};
+    TRY(qn.alloc((size_t)half * Qn.stride));
+    Qn.data = qn.p;
+    TRY(p_mul(ctx, pr, Q_even, Q_odd, Qn, "Q", n1));
+    TRY(p_compact(ctx, pr, Qn, "Q", n1));
+    BatchMPArray R_even{R.data, R.length, half, R.stride * 2};
+    BatchMPArray R_odd{R.data + R.stride, R.length, half, R.stride * 2};
+    BatchMPArray R1{nullptr, R.length + Q.length, half, R.length + Q.length};
+    TRY(r1b.alloc((size_t)half * R1.stride));
+    R1.data = r1b.p;
+    TRY(p_mul(ctx, pr, R_even, Q_odd, R1, "R*Q", n1));
+    const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
+    BatchMPArray R2{nullptr, R.length + P.length, half, R.length + P.length};
+    TRY(r2b.alloc((size_t)half * R2.stride));
+    R2.data = r2b.p;
+    P_even.batch_size = half;
+    TRY(p_mul(ctx, pr, P_even, R_odd, R2, "P*R", n1));
+    const uint32_t r1_shifted = R1.length + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
+    const uint32_t rlen = std::max(r1_shifted, R2.length) + (subtract ? 0u : 1u);
+    Rn = BatchMPArray{nullptr, rlen, half, rlen};
+    TRY(rn.alloc((size_t)half * rlen));
+    Rn.data = rn.p;
+    TRY(p_shift_addsub(ctx, pr, R1, R2, Rn, shift, subtract, n1));
+    TRY(p_compact(ctx, pr, Rn, "R", n1));
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// One merge level with shared forward transforms (the tuned form of
+// pi_bs_gpu.cu:625-723): Q_o serves Q' = Q_e Q_o and R1 = R_e Q_o, P_e
+// serves P' = P_e P_o and R2 = P_e R_o, so the level's four products take
+// six forward transforms instead of eight (four inverse either way); then
+// R' = (R1 << s) +- R2 as in the plain level.  Used when all four products
+// have the same transform shape (summing R' in the transform domain would
+// need room for R1 << s, about 6 % longer than R1, which sits just below a
+// power of two at every level and would double the transforms).  The
+// integers are those of the plain level.  *done = false (nothing issued)
+// when the level does not qualify.
+// ---------------------------------------------------------------------------
+static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, uint32_t n1, uint32_t half,
+                               uint32_t ignore, bool subtract, const BatchMPArray &P, const BatchMPArray &Q,
+                               const BatchMPArray &R, Buf &pn, BatchMPArray &Pn, Buf &qn, BatchMPArray &Qn, Buf &rn,
+                               BatchMPArray &Rn, bool *done) {
+    *done = false;
+    const uint32_t lp = P.length, lq = Q.length, lr = R.length;
+    const uint32_t pb = half - ignore;   // rows of P'
+    const SpectrumShape S = spectrum_shape((uint64_t)lr + lq - 1u);
+    if (S.M == 0 || pb == 0u) return cudaSuccess;
+    const uint64_t needs[3] = {2ull * lq - 1u, (uint64_t)lp + lr - 1u, 2ull * lp - 1u};
+    for (uint64_t nd : needs) {
+        const SpectrumShape T = spectrum_shape(nd);
+        if (T.M != S.M || T.log_k != S.log_k) return cudaSuccess;
+    }
+    *done = true;
+    const NTTPrecomputedTables &tab = context_tables(ctx);
+    const uint64_t words = spectrum_words(S, half);
+    const BatchMPArray P_even{P.data, lp, half, P.stride * 2}, P_odd{P.data + P.stride, lp, pb, P.stride * 2};
+    const BatchMPArray Q_even{Q.data, lq, half, Q.stride * 2}, Q_odd{Q.data + Q.stride, lq, half, Q.stride * 2};
+    const BatchMPArray R_even{R.data, lr, half, R.stride * 2}, R_odd{R.data + R.stride, lr, half, R.stride * 2};
+    Buf fpe, fpo, fqe, fqo, fre, fro, flags, r1b, r2b;
+    TRY(flags.alloc(spectrum_flag_words(half, std::max(std::max(lr + lq, 2u * lq), std::max(lr + lp, 2u * lp)))));
+    auto product = [&](const char *label, uint32_t rows, const Buf &fx, const Buf &fy, uint32_t *C, uint32_t Lc,
+                       uint32_t la, uint32_t lb) {
+        return stage(pr, "mul", label, n1, rows, la, lb, true, [&]() {
+            const uint32_t *X[1] = {fx.p}, *Y[1] = {fy.p};
+            spectrum_inverse(tab, S, rows, 1, X, Y, fx.p, C, Lc, Lc, flags.p);
+            return cudaGetLastError();
+        });
+    };
+    // P' = P_e P_o (P_e kept for R2)
+    TRY(stage(pr, "fwd", "P_e,P_o", n1, half, lp, lp, true, [&]() {
+        TRY(fpe.alloc(words));
+        TRY(fpo.alloc(words));
+        spectrum_forward(tab, S, half, P_even.data, P_even.stride, lp, fpe.p, nullptr, 0, 0, nullptr);
+        spectrum_forward(tab, S, pb, P_odd.data, P_odd.stride, lp, fpo.p, nullptr, 0, 0, nullptr);
+        return cudaGetLastError();
+    }));
+    Pn = BatchMPArray{nullptr, 2u * lp, pb, 2u * lp};
+    TRY(pn.alloc((size_t)pb * Pn.stride));
+    Pn.data = pn.p;
+    // P_e's spectrum is needed again for R2: the product writes into P_o's
+    TRY(stage(pr, "mul", "P", n1, pb, lp, lp, true, [&]() {
+        const uint32_t *X[1] = {fpo.p}, *Y[1] = {fpe.p};
+        spectrum_inverse(tab, S, pb, 1, X, Y, fpo.p, Pn.data, Pn.stride, Pn.length, flags.p);
+        return cudaGetLastError();
+    }));
+    fpo.reset();
+    TRY(p_compact(ctx, pr, Pn, "P", n1));
+    // Q' = Q_e Q_o (Q_o kept for R1)
+    TRY(stage(pr, "fwd", "Q_o,Q_e", n1, half, lq, lq, true, [&]() {
+        TRY(fqo.alloc(words));
+        TRY(fqe.alloc(words));
+        spectrum_forward(tab, S, half, Q_odd.data, Q_odd.stride, lq, fqo.p, Q_even.data, Q_even.stride, lq, fqe.p);
+        return cudaGetLastError();
+    }));
+    Qn = BatchMPArray{nullptr, 2u * lq, half, 2u * lq};
+    TRY(qn.alloc((size_t)half * Qn.stride));
+    Qn.data = qn.p;
+    TRY(product("Q", half, fqe, fqo, Qn.data, Qn.length, lq, lq));
+    fqe.reset();
+    TRY(p_compact(ctx, pr, Qn, "Q", n1));
+    // R1 = R_e Q_o, R2 = P_e R_o
+    TRY(stage(pr, "fwd", "R_e,R_o", n1, half, lr, lr, true, [&]() {
+        TRY(fre.alloc(words));
+        TRY(fro.alloc(words));
+        spectrum_forward(tab, S, half, R_even.data, R_even.stride, lr, fre.p, R_odd.data, R_odd.stride, lr, fro.p);
+        return cudaGetLastError();
+    }));
+    const BatchMPArray R1{nullptr, lr + lq, half, lr + lq}, R2{nullptr, lr + lp, half, lr + lp};
+    TRY(r1b.alloc((size_t)half * R1.stride));
+    TRY(r2b.alloc((size_t)half * R2.stride));
+    TRY(product("R*Q", half, fre, fqo, r1b.p, R1.length, lr, lq));
+    TRY(product("P*R", half, fro, fpe, r2b.p, R2.length, lp, lr));
+    fre.reset();
+    fro.reset();
+    fqo.reset();
+    fpe.reset();
+    const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
+    const uint32_t r1_shifted = R1.length + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
+    const uint32_t rlen = std::max(r1_shifted, R2.length) + (subtract ? 0u : 1u);
+    Rn = BatchMPArray{nullptr, rlen, half, rlen};
+    TRY(rn.alloc((size_t)half * rlen));
+    Rn.data = rn.p;
+    TRY(p_shift_addsub(ctx, pr, BatchMPArray{r1b.p, R1.length, half, R1.stride},
+                       BatchMPArray{r2b.p, R2.length, half, R2.stride}, Rn, shift, subtract, n1));
+    return p_compact(ctx, pr, Rn, "R", n1);
+}
+
 // ---------------------------------------------------------------------------
 // Binary splitting of 17N terms (pi_bs_gpu.cu:504-792).
 // Q and R (batch 1) are returned in qbuf/rbuf with their compacted lengths.
+// tuned: levels whose four products share one transform shape of at least
+// 8192 points run as tuned_level (same integers).
 // ---------------------------------------------------------------------------
 static cudaError_t binary_split(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &qbuf, BatchMPArray &Q,
-                                Buf &rbuf, BatchMPArray &R) {
+                                Buf &rbuf, BatchMPArray &R, bool tuned) {
     if (N == 0u || (N & (N - 1u)) != 0u) return cudaErrorInvalidValue;
     cudaStream_t st = current_stream();
     const uint32_t n = N * 16u;
@@ -238,52 +390,16 @@ static cudaError_t binary_split(BatchMPContext *ctx, Profiler *pr, uint32_t N, B
         const bool subtract = (n1 == n) || (n1 == (n >> 4));
         const uint32_t ignore = (n1 <= N) ? 1u : 0u;
         const uint32_t half = n1 / 2u;
-        BatchMPArray P_even{P.data, P.length, half - ignore, P.stride * 2};
-        BatchMPArray P_odd{P.data + P.stride, P.length, half - ignore, P.stride * 2};
-        BatchMPArray Pn{nullptr, P.length * 2u, half - ignore, P.length * 2u};
-        if (P_odd.batch_size > 0u) {
-            TRY(pn.alloc((size_t)Pn.batch_size * Pn.stride));
-            Pn.data = pn.p;
-            TRY(p_mul(ctx, pr, P_even, P_odd, Pn, "P", n1));
-            TRY(p_compact(ctx, pr, Pn, "P", n1));
-        } else {
-            pn.reset();
-            Pn = BatchMPArray{nullptr, 0, 0, 0};
-        }
-        BatchMPArray Q_even{Q.data, Q.length, half, Q.stride * 2};
-        BatchMPArray Q_odd{Q.data + Q.stride, Q.length, half, Q.stride * 2};
-        BatchMPArray Qn{nullptr, Q.length * 2u, half, Q.length * 2u};
-        TRY(qn.alloc((size_t)half * Qn.stride));
-        Qn.data = qn.p;
-        TRY(p_mul(ctx, pr, Q_even, Q_odd, Qn, "Q", n1));
-        TRY(p_compact(ctx, pr, Qn, "Q", n1));
-        BatchMPArray R_even{R.data, R.length, half, R.stride * 2};
-        BatchMPArray R_odd{R.data + R.stride, R.length, half, R.stride * 2};
-        BatchMPArray R1{nullptr, R.length + Q.length, half, R.length + Q.length};
-        TRY(r1b.alloc((size_t)half * R1.stride));
-        R1.data = r1b.p;
-        TRY(p_mul(ctx, pr, R_even, Q_odd, R1, "R*Q", n1));
-        const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
-        BatchMPArray R2{nullptr, R.length + P.length, half, R.length + P.length};
-        TRY(r2b.alloc((size_t)half * R2.stride));
-        R2.data = r2b.p;
-        P_even.batch_size = half;
-        TRY(p_mul(ctx, pr, P_even, R_odd, R2, "P*R", n1));
-        const uint32_t r1_shifted = R1.length + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
-        const uint32_t rlen = std::max(r1_shifted, R2.length) + (subtract ? 0u : 1u);
-        BatchMPArray Rn{nullptr, rlen, half, rlen};
-        TRY(rn.alloc((size_t)half * rlen));
-        Rn.data = rn.p;
-        TRY(p_shift_addsub(ctx, pr, R1, R2, Rn, shift, subtract, n1));
-        TRY(p_compact(ctx, pr, Rn, "R", n1));
+        BatchMPArray Pn, Qn, Rn;
+        bool done = false;
+        if (tuned) TRY(tuned_level(ctx, pr, n, n1, half, ignore, subtract, P, Q, R, pn, Pn, qn, Qn, rn, Rn, &done));
+        if (!done) TRY(plain_level(ctx, pr, n, n1, half, ignore, subtract, P, Q, R, pn, Pn, qn, Qn, rn, Rn));
         pb.swap(pn);
         qb.swap(qn);
         rb.swap(rn);
         P = Pn;
         Q = Qn;
         R = Rn;
-        r1b.reset();
-        r2b.reset();
         pn.reset();
         qn.reset();
         rn.reset();
@@ -599,14 +715,15 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
 // ---------------------------------------------------------------------------
 // pi_fractional (pi_bs_gpu.cu:1524-1685)
 // ---------------------------------------------------------------------------
-static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, Buf &retbuf, BatchMPArray &RET) {
+static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, Buf &retbuf, BatchMPArray &RET,
+                                 bool tuned) {
     cudaStream_t st = current_stream();
     uint32_t N = 1;
     while (N * 17 * 14.3 < target) N *= 2;
     const int prec = (int)(((long)(target * 3.322) + 31) / 32 + 1);
     Buf qbs, rbs;
     BatchMPArray Qbs, Rbs;
-    TRY(binary_split(ctx, pr, N, qbs, Qbs, rbs, Rbs));
+    TRY(binary_split(ctx, pr, N, qbs, Qbs, rbs, Rbs, tuned));
     const long rts = 15l * N * 17 - 8;
     const int rbits = (int)(rts % 32), rlimbs = (int)(rts / 32);
     BatchMPArray Rpre{Rbs.data + rlimbs, Rbs.length - rlimbs, 1, Rbs.length - rlimbs};
@@ -749,7 +866,7 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     BatchMPArray RET{};
     ConvertDecimalPowerTable powers{};
     char *d_digits = nullptr;
-    if (err == cudaSuccess) err = pi_fractional(ctx, &prof, (int)requested, retb, RET);
+    if (err == cudaSuccess) err = pi_fractional(ctx, &prof, (int)requested, retb, RET, req.tuned);
     // RET into the caller's buffer on a side stream, overlapping the decimal
     // conversion (which only reads RET)
     cudaStream_t side = nullptr;

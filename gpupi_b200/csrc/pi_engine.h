@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "batch_arith.h"
+#include "batch_mul_ntt.h"
 
 namespace gpupi {
 
@@ -27,6 +28,7 @@ struct PiRequest {
     char *host_digits = nullptr;    // caller buffer (>= copy_digits bytes, may be pinned) for the digits
     uint32_t *host_ret = nullptr;   // caller buffer for RET (copied while the digits are converted)
     size_t host_ret_cap = 0;        // its capacity in limbs
+    bool tuned = false;             // share forward transforms within merge levels (same results)
 };
 
 struct PiOutput {
@@ -48,6 +50,7 @@ uint32_t prec_limbs_for_digits(uint32_t digits);
 cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 // batch_mp_mul with this library's schoolbook/NTT crossover (school_max()).
 cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
+const NTTPrecomputedTables &context_tables(const BatchMPContext *ctx);
 void set_school_max(uint32_t v);
 uint32_t school_max();
 

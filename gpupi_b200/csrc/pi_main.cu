@@ -1,9 +1,11 @@
 // pi_bs_gpu command line (gpupi pi_bs_gpu.cu:2073-2437, main_fractional).
 //
-//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print]
+//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print] [--tuned]
 //
 // Same arguments, stdout/stderr lines and exit codes as the reference; the
-// computation is gpupi_b200's pipeline (pi_engine.cu).
+// computation is gpupi_b200's pipeline (pi_engine.cu).  --tuned (an addition)
+// shares forward transforms within each merge level instead of the
+// reference's op sequence; both print the same RET and digits.
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -64,7 +66,7 @@ void hex_preview(const char *label, const uint32_t *limbs, uint32_t length) {   
 }
 
 void usage(const char *prog) {
-    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print]\n", prog);
+    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--tuned]\n", prog);
 }
 
 }  // namespace
@@ -81,18 +83,22 @@ int main(int argc, char **argv) {
         return 1;
     }
     const uint32_t requested = (uint32_t)target;
-    bool benchmark = false, profile = false, full = false;
-    if (argc >= 3) {
-        if (strcmp(argv[2], "--benchmark") == 0) benchmark = true;
-        else if (strcmp(argv[2], "--profile-stages") == 0) profile = true;
-        else if (strcmp(argv[2], "--full-print") == 0) full = true;
-        else {
-            usage(argv[0]);
-            return 1;
-        }
+    bool benchmark = false, profile = false, full = false, tuned = false;
+    int modes = 0;
+    for (int i = 2; i < argc; ++i) {
+        if (strcmp(argv[i], "--benchmark") == 0) benchmark = true, ++modes;
+        else if (strcmp(argv[i], "--profile-stages") == 0) profile = true, ++modes;
+        else if (strcmp(argv[i], "--full-print") == 0) full = true, ++modes;
+        else if (strcmp(argv[i], "--tuned") == 0 && !tuned) tuned = true;
+        else modes = 2;
+    }
+    if (modes > 1) {
+        usage(argv[0]);
+        return 1;
     }
     gpupi::PiRequest req;
     req.digits = requested;
+    req.tuned = tuned;
     req.profile_stages = profile;
     if (benchmark) req.copy_digits = std::min<uint32_t>(requested, 63u);
     else if (profile) req.copy_digits = std::min<uint32_t>(requested, 4096u);

@@ -1,0 +1,45 @@
+// Products that share forward transforms (mul_ntt.cu).
+//
+// A spectrum is the complete forward transform of N rows at one shape
+// (N * M * 3 * K residues).  Operands transformed once serve every product
+// they take part in, and a sum of products costs one inverse transform:
+//   spectrum_forward(X) ; spectrum_forward(Y) ; ...
+//   spectrum_inverse(sum_t X_t Y_t) -> limbs.
+// The result is the exact integer sum, provided spectrum_sum_fits() holds
+// for the operand lengths and the shape covers the output's L_c - 1
+// coefficients (spectrum_shape(L_c - 1)).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "batch_mul_ntt.h"
+
+namespace gpupi {
+
+struct SpectrumShape {
+    int log_k;   // K = 2^log_k points per coset
+    int M;       // cosets; 0 = no shared-transform path for this size
+};
+
+// Shape for outputs of up to ncoef coefficients; M = 0 below 8192 points
+// (one fused kernel per product) and above 2^28 points.
+SpectrumShape spectrum_shape(uint64_t ncoef);
+uint64_t spectrum_words(SpectrumShape s, uint32_t N);        // N * M * 3 * K
+uint64_t spectrum_flag_words(uint32_t N, uint32_t Lc);       // carry flags of spectrum_inverse
+// CRT capacity: sum_t min(La_t, Lb_t) (2^32 - 1)^2 < p0 p1 p2.
+bool spectrum_sum_fits(const uint32_t *La, const uint32_t *Lb, int terms);
+
+// FX (and FY when Y is not null) = forward transforms of N rows of X (Y);
+// rows at X + i * sX, Lx limbs (zero above).
+void spectrum_forward(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, const uint32_t *X,
+                      uint64_t sX, uint32_t Lx, uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly,
+                      uint32_t *FY);
+// C rows (stride sC, Lc limbs) = sum over terms (<= 2) of X_t Y_t.  Fout
+// receives the intermediate residues and may be one of the X_t / Y_t;
+// flags: spectrum_flag_words(N, Lc) words.
+void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, int terms,
+                      const uint32_t *const *X, const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC,
+                      uint32_t Lc, uint32_t *flags);
+
+}  // namespace gpupi

@@ -107,9 +107,25 @@ int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *d_X, uint32_t L_x, uin
  * may be null.  info[0..7] receives: convert_digits, RET length, elapsed ms
  * on the device (float bits), workspace MB, number of profiled stages, leaf
  * digits, 0, 0.  flags bit 0 = profile every stage, bit 1 = keep RET and the
- * digits on the device (no host copies). */
+ * digits on the device (no host copies), bit 2 = tuned form: forward
+ * transforms shared within each merge level of the splitting tree and R'
+ * summed in the transform domain (the default is the reference's op
+ * sequence, one batched product per op; both give the same RET and
+ * digits). */
 int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
                      char *h_digits, size_t digits_cap, uint32_t *info);
+
+/* C = A B, or A B + D E when D is not null, through shared-transform
+ * spectra: each operand's forward transform is computed once and the sum
+ * costs one inverse transform (the building block of the tuned form of the
+ * splitting tree).  N rows, each operand and C packed (stride = length);
+ * Lc >= La + Lb (and >= Ld + Le + 1).  cudaErrorInvalidValue when the
+ * product is below 8192 transform points, above 2^28, or when
+ * min(La, Lb) + min(Ld, Le) limbs of 32-bit products would exceed the
+ * three-prime CRT capacity.  No counterpart in the reference. */
+int gpupi_mp_mul_spectra(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, const uint32_t *B,
+                         uint32_t Lb, const uint32_t *D, uint32_t Ld, const uint32_t *E, uint32_t Le, uint32_t *C,
+                         uint32_t Lc);
 
 /* Per-kernel timing: CUDA events around each launch on the current stream,
  * with the launch's algorithmic HBM bytes.  The report has one line per

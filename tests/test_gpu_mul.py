@@ -171,3 +171,42 @@ def test_ragged_large_and_single(ctx):
     rng = np.random.default_rng(7)
     _ragged_case(ctx, [70000, 3, 130000], [50000, 90000, 1], rng)
     _ragged_case(ctx, [1], [1], rng)
+
+
+def _int_rows(buf, N, L):
+    out = []
+    for r in range(N):
+        out.append(int.from_bytes(buf[r * L:(r + 1) * L].astype("<u4").tobytes(), "little"))
+    return out
+
+
+@pytest.mark.parametrize("N,La,Lb,Ld,Le", [(3, 5000, 4000, 4500, 4499), (1, 40000, 50000, 60000, 30000),
+                                           (2, 100000, 1, 3, 100000)])
+def test_spectra_products_and_sums(ctx, N, La, Lb, Ld, Le):
+    """Shared-transform spectra: A B and A B + D E (one inverse transform for
+    the sum) equal the exact integers."""
+    rng = np.random.default_rng(N * 7 + La + Le)
+    A, B = rand_buf(rng, N, La, La), rand_buf(rng, N, Lb, Lb)
+    D, E = rand_buf(rng, N, Ld, Ld), rand_buf(rng, N, Le, Le)
+    Lc1 = La + Lb
+    Lc2 = max(La + Lb, Ld + Le + 1)
+    dA, dB, dD, dE = to_dev(A), to_dev(B), to_dev(D), to_dev(E)
+    C1 = to_dev(np.zeros(N * Lc1, dtype=np.uint32))
+    C2 = to_dev(np.zeros(N * Lc2, dtype=np.uint32))
+    ctx.mul_spectra(N, dA.ptr, La, dB.ptr, Lb, C1.ptr, Lc1)
+    ctx.mul_spectra(N, dA.ptr, La, dB.ptr, Lb, C2.ptr, Lc2, dD.ptr, Ld, dE.ptr, Le)
+    a, b, d, e = _int_rows(A, N, La), _int_rows(B, N, Lb), _int_rows(D, N, Ld), _int_rows(E, N, Le)
+    c1, c2 = _int_rows(C1.numpy(), N, Lc1), _int_rows(C2.numpy(), N, Lc2)
+    for r in range(N):
+        assert c1[r] == a[r] * b[r]
+        assert c2[r] == a[r] * b[r] + d[r] * e[r]
+
+
+def test_spectra_rejects_small_and_overflowing(ctx):
+    """Below 8192 transform points the shared-transform path does not apply."""
+    import gpupi_b200 as g
+    rng = np.random.default_rng(5)
+    A = to_dev(rand_buf(rng, 1, 100, 100))
+    C = to_dev(np.zeros(200, dtype=np.uint32))
+    with pytest.raises(g.GpupiError):
+        ctx.mul_spectra(1, A.ptr, 100, A.ptr, 100, C.ptr, 200)
