@@ -2,7 +2,7 @@
 // API batch_mul_ntt.h:24-40).
 //
 // Shape.  A product of L_c = L_a + L_b limbs is a cyclic convolution of
-// M * K points, K = 2^k <= 2^25, M <= 8, M * K >= L_a + L_b - 1.  M = 1 for
+// M * K points, K = 2^k <= 2^25, M <= 20, M * K >= L_a + L_b - 1.  M = 1 for
 // products up to 2^25 points.  Longer products are split into M cosets:
 // with c_i = g^(iK) (g a generator, i < M) the residues
 // C_i = A B mod (x^K - c_i) are K-point cyclic convolutions of the twisted
@@ -202,8 +202,8 @@ __device__ __forceinline__ void load_limbs(const ColsArgs &a, uint32_t (&x)[16],
             uint32_t pos, c;
             First::elem(t, 0, pos, c);
             const uint32_t i0 = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
-            uint32_t f = mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset * i0);
-            const uint32_t d = mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << (First::kLO + log_cols));
+            uint32_t f = mul_coset<Q, 0>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset * i0);
+            const uint32_t d = mul_coset<Q, 0>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << (First::kLO + log_cols));
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 x[j] = norm<Q>(mont<Q>(x[j], f));
@@ -215,7 +215,7 @@ __device__ __forceinline__ void load_limbs(const ColsArgs &a, uint32_t (&x)[16],
                 uint32_t pos, c;
                 First::elem(t, j, pos, c);
                 const uint32_t i = (uint32_t)(((uint64_t)pos << log_cols) + c0 + c);
-                x[j] = mul_coset<Q>(x[j], clo, chi, (uint32_t)coset * i);
+                x[j] = mul_coset<Q, 0>(x[j], clo, chi, (uint32_t)coset * i);
             }
         }
     }
@@ -268,7 +268,7 @@ __device__ __forceinline__ void cols_body(const NttParams &P, const ColsArgs &a,
         const uint32_t *clo = coset_lo_ptr(P.tab, 0, Q);
         const uint32_t *chi = coset_hi_ptr(P.tab, 0, Q);
         // coset node c = g^(coset K), Montgomery form
-        const uint32_t cm = (a.M > 1) ? mul_coset<Q>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << a.log_k) : 0u;
+        const uint32_t cm = (a.M > 1) ? mul_coset<Q, 0>(PrimeC<Q>::r1, clo, chi, (uint32_t)coset << a.log_k) : 0u;
         load_limbs<First, LOG_R, Q>(a, x, a.X + row * a.sX, a.Lx, a.nb, K, log_cols, c0, t, coset, cm, clo, chi);
         if constexpr (PAIR)
             load_limbs<First, LOG_R, Q>(a, y, a.X2 + row * a.sX2, a.Lx2, a.nb2, K, log_cols, c0, t, coset, cm, clo,
@@ -613,7 +613,7 @@ __device__ __forceinline__ void combine_body(const NttParams &P, const CombineAr
     uint32_t u[M];
     u[0] = F0[0];
 #pragma unroll
-    for (int i = 1; i < M; ++i) u[i] = mul_coset<Q>(F0[(uint64_t)i * 3 * K], clo, chi, (uint32_t)i * j);
+    for (int i = 1; i < M; ++i) u[i] = mul_coset<Q, 1>(F0[(uint64_t)i * 3 * K], clo, chi, (uint32_t)i * j);
 #pragma unroll
     for (int b = 0; b < M; ++b) {
         uint32_t acc = 0u;
@@ -939,6 +939,14 @@ static int column_passes(int log_k, int (&passes)[2]) {
     return 2;
 }
 
+// Every coefficient, at most min(L_a, L_b) (2^32 - 1)^2, is below p0 p1 p2
+// (min(L_a, L_b) < 4.18e8).
+static bool crt_fits(uint64_t min_len) {
+    unsigned __int128 cap = 1;
+    for (int q = 0; q < kPrimes; ++q) cap *= kP[q];
+    return (unsigned __int128)min_len * 0xffffffffull * 0xffffffffull < cap;
+}
+
 static void launch_combine(int M, const NttParams &P, const CombineArgs &c, uint32_t N, cudaStream_t st) {
     const uint64_t K = 1ull << c.log_k;
     const unsigned blocks = (unsigned)((uint64_t)N * kPrimes * (K / kThreads));
@@ -950,7 +958,19 @@ static void launch_combine(int M, const NttParams &P, const CombineArgs &c, uint
         case 5: k_combine<5><<<blocks, kThreads, 0, st>>>(P, c); break;
         case 6: k_combine<6><<<blocks, kThreads, 0, st>>>(P, c); break;
         case 7: k_combine<7><<<blocks, kThreads, 0, st>>>(P, c); break;
-        default: k_combine<8><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 8: k_combine<8><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 9: k_combine<9><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 10: k_combine<10><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 11: k_combine<11><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 12: k_combine<12><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 13: k_combine<13><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 14: k_combine<14><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 15: k_combine<15><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 16: k_combine<16><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 17: k_combine<17><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 18: k_combine<18><<<blocks, kThreads, 0, st>>>(P, c); break;
+        case 19: k_combine<19><<<blocks, kThreads, 0, st>>>(P, c); break;
+        default: k_combine<20><<<blocks, kThreads, 0, st>>>(P, c); break;
     }
     count_launch();
 }
@@ -975,7 +995,11 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
     }
     const Shape s = shape_for(La, Lb);
     if (s.M > kMaxCosets) {
-        fprintf(stderr, "gpupi_b200: product of %u limbs exceeds the 2^28-point limit\n", Lc);
+        fprintf(stderr, "gpupi_b200: product of %u limbs exceeds the 20 * 2^25-point limit\n", Lc);
+        return;
+    }
+    if (!crt_fits(La < Lb ? La : Lb)) {
+        fprintf(stderr, "gpupi_b200: min(L_a, L_b) = %u exceeds the three-prime CRT capacity\n", La < Lb ? La : Lb);
         return;
     }
     const int log_k = s.log_k, M = s.M;

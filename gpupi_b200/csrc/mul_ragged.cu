@@ -146,7 +146,7 @@ cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const
     for (uint32_t i = 0; i < N; ++i) {
         const RaggedRow d{offA[i], offB[i], offC[i], La[i], Lb[i]};
         const uint64_t Lc = (uint64_t)d.La + d.Lb;
-        if (Lc > (1ull << 28)) return cudaErrorInvalidValue;
+        if (Lc > (20ull << 25) || std::min(d.La, d.Lb) > (1u << 28)) return cudaErrorInvalidValue;
         if (d.La == 0u || d.Lb == 0u) {
             zero.push_back(d);
         } else if (Lc <= school_max()) {

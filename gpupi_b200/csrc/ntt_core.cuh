@@ -31,7 +31,8 @@ constexpr uint32_t kLoSize = 1u << kLoBits;
 constexpr uint32_t kHiSize = 1u << (kMaxLog - kLoBits);   // 4096
 constexpr int kCosetLoBits = 14;     // coset tables: g^e for e < 2^28
 constexpr uint32_t kCosetSize = 1u << kCosetLoBits;
-constexpr int kMaxCosets = 8;
+constexpr int kMaxCosets = 20;   // products up to 20 * 2^25 limbs
+static_assert((uint64_t)kMaxCosets << 25 <= 3ull << 28, "coset exponents below 3 * 2^28");
 
 constexpr uint32_t inv_2_32(uint32_t p) {
     uint32_t x = p;   // Newton iteration for p^-1 mod 2^32
@@ -65,12 +66,33 @@ template <>
 struct Prime<2> {
     static constexpr uint32_t p = 2113929217u, g = 5u;
 };
+// b^e mod p (host and compile time)
+constexpr uint32_t cpow(uint64_t b, uint64_t e, uint64_t p) {
+    uint64_t r = 1u % p;
+    b %= p;
+    while (e) {
+        if (e & 1u) r = r * b % p;
+        b = b * b % p;
+        e >>= 1;
+    }
+    return (uint32_t)r;
+}
+
 template <int Q>
 struct PrimeC {
     static constexpr uint32_t p = Prime<Q>::p;
     static constexpr uint32_t pinv = inv_2_32(p);
     static constexpr uint32_t r1 = (uint32_t)((1ull << 32) % p);   // R mod p: Montgomery form of 1
+    // Montgomery forms of g^(+-k 2^28), k = 1, 2: coset exponents reach 20 * 2^25
+    static constexpr uint32_t g28 = (uint32_t)(((uint64_t)cpow(Prime<Q>::g, 1ull << 28, p) << 32) % p);
+    static constexpr uint32_t g29 = (uint32_t)(((uint64_t)cpow(Prime<Q>::g, 1ull << 29, p) << 32) % p);
+    static constexpr uint32_t g28inv =
+        (uint32_t)(((uint64_t)cpow(Prime<Q>::g, (p - 1ull) - ((1ull << 28) % (p - 1ull)), p) << 32) % p);
+    static constexpr uint32_t g29inv =
+        (uint32_t)(((uint64_t)cpow(Prime<Q>::g, (p - 1ull) - ((1ull << 29) % (p - 1ull)), p) << 32) % p);
 };
+static_assert((uint64_t)cpow(13, 1ull << 28, 1811939329u) * cpow(13, 1811939328ull - (1ull << 28), 1811939329u) %
+                      1811939329u == 1u, "g^(2^28) g^(-2^28) = 1");
 static_assert(PrimeC<0>::p * PrimeC<0>::pinv == 1u, "p0 inverse");
 static_assert(PrimeC<1>::p * PrimeC<1>::pinv == 1u, "p1 inverse");
 static_assert(PrimeC<2>::p * PrimeC<2>::pinv == 1u, "p2 inverse");
@@ -114,7 +136,8 @@ __device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b) {
 //                               h = 2^lh, m < h, lh < 12: the twiddles of
 //                               radix-2 level lh, contiguous per level
 //   lv2: COSET_LO[dir][q][2^14] g^e, COSET_HI[dir][q][2^14] g^(e 2^14), Montgomery
-//        form, dir 1 holds g^-1 (coset twists beta_i^j = g^(i j), i j < 2^28)
+//        form, dir 1 holds g^-1 (coset twists beta_i^j = g^(i j), i j < 20 2^25:
+//        the bits above 2^28 through PrimeC::g28 / g29 and inverses)
 //   inv2n: [k][q]  2^-k * R^2 mod p (scale of the pointwise product)
 constexpr int kLevelLogMax = 12;
 constexpr uint32_t kLevelSize = (1u << kLevelLogMax) - 1u;        // 4095
@@ -163,9 +186,18 @@ template <int Q>
 __device__ __forceinline__ uint32_t root_m(const uint2 *lo, const uint2 *hi, uint32_t E) {
     return mul_root<Q>(PrimeC<Q>::r1, lo, hi, E);
 }
-// x * g^(+-E) for E < 2^28, result in [0, p)
-template <int Q>
+// x * g^E (DIR 0) or x * g^-E (DIR 1, lo / hi the dir-1 tables) for
+// E < 3 * 2^28, result in [0, p); the tables cover E < 2^28, the top bits
+// are one more product.
+template <int Q, int DIR>
 __device__ __forceinline__ uint32_t mul_coset(uint32_t x, const uint32_t *lo, const uint32_t *hi, uint32_t E) {
+    const uint32_t top = E >> 28;
+    if (top) {
+        const uint32_t f = DIR ? (top == 1u ? PrimeC<Q>::g28inv : PrimeC<Q>::g29inv)
+                               : (top == 1u ? PrimeC<Q>::g28 : PrimeC<Q>::g29);
+        x = norm<Q>(mont<Q>(x, f));
+        E &= (1u << 28) - 1u;
+    }
     const uint32_t a = __ldg(lo + (E & (kCosetSize - 1u)));
     const uint32_t b = __ldg(hi + (E >> kCosetLoBits));
     return norm<Q>(mont<Q>(mont<Q>(x, a), b));

@@ -811,6 +811,8 @@ uint32_t round_up_decimal_digits(uint32_t requested, uint32_t *leaf_out) {
     return digits << levels;
 }
 
+constexpr uint32_t kMaxDigits = 1290000000u;   // digits * 3.322 + 31 < 2^32
+
 uint32_t prec_limbs_for_digits(uint32_t digits) {
     const uint32_t bits = (uint32_t)((double)digits * 3.322) + 31u;   // pi_bs_gpu.cu:941-944
     return bits / 32u + 1u;
@@ -828,6 +830,12 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     out.target_digits = requested;
     out.convert_digits = convert;
     if (requested > 0u && convert == 0u) return cudaErrorInvalidValue;
+    // The working precision in bits (digits * 3.322 + 31, pi_bs_gpu.cu:941-944)
+    // is a 32-bit count.  Up to 1.011e9 digits the splitting tree has 2^22 x
+    // 17 terms and its products stay below the reference's 2^28-limb NTT
+    // ceiling; above that the tree doubles and its top products (about 5.5e8
+    // limbs) need this library's 20-coset transforms.
+    if (requested > kMaxDigits) return cudaErrorInvalidValue;
     BatchMPContext *ctx = req.ctx;
     bool own_ctx = false;
     if (!ctx) {

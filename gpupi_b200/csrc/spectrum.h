@@ -23,7 +23,7 @@ struct SpectrumShape {
 };
 
 // Shape for outputs of up to ncoef coefficients; M = 0 below 8192 points
-// (one fused kernel per product) and above 2^28 points.
+// (one fused kernel per product) and above 20 * 2^25 points.
 SpectrumShape spectrum_shape(uint64_t ncoef);
 uint64_t spectrum_words(SpectrumShape s, uint32_t N);        // N * M * 3 * K
 uint64_t spectrum_flag_words(uint32_t N, uint32_t Lc);       // carry flags of spectrum_inverse

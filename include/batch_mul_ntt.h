@@ -19,7 +19,8 @@ struct NTTPrecomputedTables {
 void init_ntt_precomputed_tables(NTTPrecomputedTables *tables);
 
 // ret = A * B for N pairs; ret rows have L_a + L_b limbs.  workspace must hold
-// batch_mul_ntt_workspace_size(N, L_a, L_b) bytes.  Product length up to 2^28 limbs.
+// batch_mul_ntt_workspace_size(N, L_a, L_b) bytes.  Product length up to 20 * 2^25 limbs
+// (the reference stops at 2^28) with min(L_a, L_b) < 4.18e8 (CRT capacity).
 void batch_mul_ntt(uint32_t *A, uint32_t *B, uint32_t *ret, uint32_t *workspace,
                    NTTPrecomputedTables tables, uint32_t N, uint32_t L_a, uint32_t L_b,
                    uint32_t stride_A, uint32_t stride_B, uint32_t stride_ret);

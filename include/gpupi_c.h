@@ -85,7 +85,7 @@ int gpupi_mul_ntt(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a,
  * C[offC[i] .. + L_a[i] + L_b[i]).  d_A, d_B, d_C are device pointers; the
  * offset and length arrays are host arrays of N entries.  Products are bucketed
  * (schoolbook in one launch, NTT per transform size) so N uneven products cost
- * a few launches instead of N calls.  L_a[i] + L_b[i] <= 2^28. */
+ * a few launches instead of N calls.  L_a[i] + L_b[i] <= 20 * 2^25, min(L_a[i], L_b[i]) <= 2^28. */
 int gpupi_mp_mul_ragged(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, const uint64_t *offA, const uint32_t *L_a,
                         const uint32_t *d_B, const uint64_t *offB, const uint32_t *L_b, uint32_t *d_C,
                         const uint64_t *offC);
@@ -120,7 +120,7 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
  * costs one inverse transform (the building block of the tuned form of the
  * splitting tree).  N rows, each operand and C packed (stride = length);
  * Lc >= La + Lb (and >= Ld + Le + 1).  cudaErrorInvalidValue when the
- * product is below 8192 transform points, above 2^28, or when
+ * product is below 8192 transform points, above 20 * 2^25, or when
  * min(La, Lb) + min(Ld, Le) limbs of 32-bit products would exceed the
  * three-prime CRT capacity.  No counterpart in the reference. */
 int gpupi_mp_mul_spectra(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t La, const uint32_t *B,

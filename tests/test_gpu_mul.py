@@ -121,6 +121,46 @@ def test_ntt_cosets(ctx):
     _check_mul(ctx, 1, L, L, L, L, 2 * L, rng, path="ntt", extreme=True)
 
 
+def _all_ones_product(a, b):
+    """Limbs of (2^(32a) - 1)(2^(32b) - 1), a >= b >= 1."""
+    c = np.full(a + b, 0xFFFFFFFF, dtype=np.uint32)
+    c[0] = 1
+    c[1:b] = 0
+    c[a] = 0xFFFFFFFE
+    return c
+
+
+def test_all_ones_product_formula():
+    for a, b in [(1, 1), (3, 2), (5, 2), (4, 4), (6, 3), (9, 1)]:
+        v = ((1 << (32 * a)) - 1) * ((1 << (32 * b)) - 1)
+        assert int.from_bytes(_all_ones_product(a, b).astype("<u4").tobytes(), "little") == v
+
+
+def test_ntt_cosets_beyond_2_28(ctx):
+    """Products past the reference's 2^28-limb ceiling: M = 9 (one long
+    operand folded over nine blocks, exact Python check) and M = 20, the
+    largest shape, on all-ones operands (the largest coefficients; coset
+    exponents up to 19 * 2^25, above 2^28 and 2^29 through constant factors),
+    checked against the closed form."""
+    rng = np.random.default_rng(30)
+    La, Lb = (1 << 28) + (1 << 24), 3                          # M = 9
+    A = rng.integers(0, 1 << 32, size=La, dtype=np.uint64).astype(np.uint32)
+    B = np.array([0xFFFFFFFF, 0x12345678, 0x9ABCDEF1], dtype=np.uint32)
+    dA, dB = to_dev(A), to_dev(B)
+    dC = to_dev(np.full(La + Lb, 0xA5A5A5A5, dtype=np.uint32))
+    ctx.mul_ntt(1, dA.ptr, La, La, dB.ptr, Lb, Lb, dC.ptr, La + Lb)
+    a = int.from_bytes(A.astype("<u4").tobytes(), "little")
+    b = int.from_bytes(B.astype("<u4").tobytes(), "little")
+    assert int.from_bytes(dC.numpy().astype("<u4").tobytes(), "little") == a * b
+    del A, dA, dC, a
+    La, Lb = 1 << 28, (20 << 25) - (1 << 28)                   # M = 20
+    dA = to_dev(np.full(La, 0xFFFFFFFF, dtype=np.uint32))
+    dB = to_dev(np.full(Lb, 0xFFFFFFFF, dtype=np.uint32))
+    dC = to_dev(np.zeros(La + Lb, dtype=np.uint32))
+    ctx.mul_ntt(1, dB.ptr, Lb, Lb, dA.ptr, La, La, dC.ptr, La + Lb)
+    assert np.array_equal(dC.numpy(), _all_ones_product(Lb, La))
+
+
 def test_ntt_cosets_broadcast_and_square(ctx):
     """Coset products with a stride-0 B (transformed once for all rows) and a squaring."""
     rng = np.random.default_rng(29)

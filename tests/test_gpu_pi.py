@@ -96,3 +96,22 @@ def test_plain_and_tuned_forms_agree(ctx, digits):
     assert tuned.ret_len == plain.ret_len
     assert np.array_equal(tuned.ret, plain.ret)
     assert tuned.dec == plain.dec
+
+
+def test_pi_beyond_the_reference_ceiling(ctx):
+    """1.2e9 digits: the splitting tree for 2^23 x 17 terms, whose top
+    products (about 5.5e8 limbs) exceed the reference's 2^28-limb NTT ceiling
+    and run on 17 cosets.  Its digits must agree with the 1e9-digit run on the
+    first 1e9 - 64 digits, and RET with BBP at seeded positions."""
+    import random
+    import gpupi_b200 as g
+    small = g.pi_compute(1_000_000_000, ctx)
+    big = g.pi_compute(1_200_000_000, ctx)
+    n = 1_000_000_000 - 64
+    assert big.dec[:n] == small.dec[:n]
+    assert big.ret_len > small.ret_len
+    rng = random.Random(0x12E9)
+    top = 8 * (big.ret_len - 1) - 64
+    positions = sorted(rng.randrange(0, min(top, 1 << 30)) for _ in range(8))
+    bad, unsure = g.bbp_spot_check(big.ret, positions)
+    assert not bad and not unsure
