@@ -68,7 +68,10 @@ _SIGS = [
     ("gpupi_bbp_fractions", ctypes.c_int, [_p, _u32, _p]),
     ("gpupi_mp_mul_ragged", ctypes.c_int, [_p, _u32, _p, _p, _p, _p, _p, _p, _p, _p]),
     ("gpupi_mp_mul_spectra", ctypes.c_int, [_p, _u32, _p, _u32, _p, _u32, _p, _u32, _p, _u32, _p, _u32]),
+    ("gpupi_pi_stream", ctypes.c_int, [_p, _u32, _u32, _p, _p, ctypes.c_size_t, _p]),
 ]
+
+_DIGIT_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
 
 C_ABI_SYMBOLS = [s[0] for s in _SIGS]
 
@@ -377,6 +380,45 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
     dec = dbuf.raw[:copy_digits].decode("ascii") if dbuf is not None else ""
     return PiResult(digits, info[0], ret_len, float(elapsed), info[3],
                     ret[:ret_len] if ret_capacity else None, dec, info[5])
+
+
+def pi_stream(digits: int, write, ctx: Context | None = None, chunk: int = 0, tuned: bool = False) -> PiResult:
+    """Compute pi to ``digits`` digits and pass the digits after "3." to
+    ``write(bytes)`` in order, in chunks of at most ``chunk`` bytes (0: 64 MiB),
+    each chunk's device-to-host copy overlapping the previous write
+    (gpupi_pi_stream).  ``write`` returning False stops the output.
+    Returns the result without RET or digits; ``output_ms`` is the host time
+    of the output."""
+    _torch()
+    failed = []
+
+    def _sink(data, n, user):
+        try:
+            return 1 if write(ctypes.string_at(data, n)) is False else 0
+        except Exception as e:   # surfaced after the call
+            failed.append(e)
+            return 1
+
+    cb = _DIGIT_SINK(_sink)
+    info = (_u32 * 8)()
+    rc = lib().gpupi_pi_stream(ctx.h if ctx else None, digits, 4 if tuned else 0,
+                               ctypes.cast(cb, ctypes.c_void_p), None, chunk, info)
+    if failed:
+        raise failed[0]
+    _check(rc, "gpupi_pi_stream")
+    elapsed = np.frombuffer(np.uint32(info[2]).tobytes(), dtype=np.float32)[0]
+    r = PiResult(digits, info[0], info[1], float(elapsed), info[3], None, "", info[5])
+    r.output_ms = float(np.frombuffer(np.uint32(info[6]).tobytes(), dtype=np.float32)[0])
+    return r
+
+
+def pi_to_file(digits: int, path, ctx: Context | None = None, chunk: int = 0, tuned: bool = False) -> PiResult:
+    """Write "3<digits>\\n" to ``path`` (the CLI's output), streamed."""
+    with open(path, "wb") as f:
+        f.write(b"3")
+        r = pi_stream(digits, f.write, ctx, chunk, tuned)
+        f.write(b"\n")
+    return r
 
 
 # ---------------------------------------------------------------------------

@@ -200,6 +200,45 @@ int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *X, uint32_t Lx, uint32
     return (int)err;
 }
 
+namespace {
+struct StreamSink {
+    gpupi_digit_sink fn;
+    void *user;
+};
+}  // namespace
+
+int gpupi_pi_stream(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, gpupi_digit_sink sink, void *user,
+                    size_t chunk, uint32_t *info) {
+    if (!sink) return (int)cudaErrorInvalidValue;
+    StreamSink k{sink, user};
+    gpupi::PiRequest req;
+    req.digits = digits;
+    req.ctx = raw(ctx);
+    req.tuned = (flags & 4u) != 0u;
+    req.sink = [](const char *data, size_t n, void *u) {
+        StreamSink *s = static_cast<StreamSink *>(u);
+        return s->fn(data, n, s->user) == 0;
+    };
+    req.sink_user = &k;
+    if (chunk) req.sink_chunk = chunk;
+    gpupi::PiOutput out;
+    const cudaError_t err = gpupi::pi_run(req, out);
+    if (err != cudaSuccess) return (int)err;
+    if (info) {
+        uint32_t leaf = 0u;
+        gpupi::round_up_decimal_digits(digits, &leaf);
+        info[0] = out.convert_digits;
+        info[1] = out.ret_len;
+        memcpy(&info[2], &out.elapsed_ms, 4);
+        info[3] = (uint32_t)(out.workspace_bytes >> 20);
+        info[4] = 0u;
+        info[5] = leaf;
+        memcpy(&info[6], &out.output_ms, 4);
+        info[7] = 0u;
+    }
+    return 0;
+}
+
 int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
                      char *h_digits, size_t digits_cap, uint32_t *info) {
     gpupi::PiRequest req;

@@ -21,6 +21,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -813,6 +814,46 @@ uint32_t round_up_decimal_digits(uint32_t requested, uint32_t *leaf_out) {
 
 constexpr uint32_t kMaxDigits = 1290000000u;   // digits * 3.322 + 31 < 2^32
 
+// Digits [0, total) of d_digits to sink in chunks: the copy of chunk i + 1
+// into one pinned buffer runs while the sink consumes chunk i from the other.
+static cudaError_t stream_digits(const char *d_digits, size_t total, const PiRequest &req, float *host_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const size_t chunk = std::max<size_t>(req.sink_chunk, 4096u);
+    char *h[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t cs = nullptr;
+    cudaError_t err = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && err == cudaSuccess; ++i) {
+        err = cudaHostAlloc((void **)&h[i], std::min(chunk, std::max<size_t>(total, 1u)), cudaHostAllocDefault);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    }
+    auto issue = [&](size_t k) {
+        const size_t off = k * chunk, n = std::min(chunk, total - off);
+        cudaError_t e = cudaMemcpyAsync(h[k & 1], d_digits + off, n, cudaMemcpyDeviceToHost, cs);
+        note_d2h(n);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k & 1], cs);
+        return e;
+    };
+    const size_t chunks = (total + chunk - 1) / chunk;
+    if (err == cudaSuccess && chunks) err = issue(0);
+    for (size_t k = 0; k < chunks && err == cudaSuccess; ++k) {
+        if (k + 1 < chunks) err = issue(k + 1);   // its buffer's previous chunk was consumed at k - 1
+        if (err == cudaSuccess) err = cudaEventSynchronize(ev[k & 1]);
+        const size_t n = std::min(chunk, total - k * chunk);
+        if (err == cudaSuccess && !req.sink(h[k & 1], n, req.sink_user)) break;
+    }
+    if (cs) {
+        cudaStreamSynchronize(cs);
+        cudaStreamDestroy(cs);
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (h[i]) cudaFreeHost(h[i]);
+        if (ev[i]) cudaEventDestroy(ev[i]);
+    }
+    *host_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return err;
+}
+
 uint32_t prec_limbs_for_digits(uint32_t digits) {
     const uint32_t bits = (uint32_t)((double)digits * 3.322) + 31u;   // pi_bs_gpu.cu:941-944
     return bits / 32u + 1u;
@@ -933,6 +974,8 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
             err = cudaMemcpyAsync(&out.tail[0], d_digits + (requested - tail), tail, cudaMemcpyDeviceToHost, st);
         }
         if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+        if (err == cudaSuccess && req.sink && requested > 0u)
+            err = stream_digits(d_digits, requested, req, &out.output_ms);
     }
     if (side) {
         const cudaError_t serr = cudaStreamSynchronize(side);

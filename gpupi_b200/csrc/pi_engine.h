@@ -29,6 +29,13 @@ struct PiRequest {
     uint32_t *host_ret = nullptr;   // caller buffer for RET (copied while the digits are converted)
     size_t host_ret_cap = 0;        // its capacity in limbs
     bool tuned = false;             // share forward transforms within merge levels (same results)
+    // Streamed digit output: after the timed region the requested digits are
+    // handed to sink in order, in chunks of at most sink_chunk bytes; each
+    // chunk's device-to-host copy (two pinned buffers, one copy stream)
+    // overlaps the sink call of the chunk before.  A false return stops.
+    bool (*sink)(const char *data, size_t n, void *user) = nullptr;
+    void *sink_user = nullptr;
+    size_t sink_chunk = (size_t)64 << 20;
 };
 
 struct PiOutput {
@@ -36,6 +43,7 @@ struct PiOutput {
     uint32_t convert_digits = 0;
     uint32_t ret_len = 0;
     float elapsed_ms = 0.f;
+    float output_ms = 0.f;          // host time of the streamed output (sink set)
     size_t workspace_bytes = 0;
     std::vector<uint32_t> ret;      // RET limbs (little endian)
     std::string digits;             // first copy_digits digits (unless PiRequest::host_digits)

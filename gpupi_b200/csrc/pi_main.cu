@@ -1,11 +1,14 @@
 // pi_bs_gpu command line (gpupi pi_bs_gpu.cu:2073-2437, main_fractional).
 //
-//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print] [--tuned]
+//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE]
 //
 // Same arguments, stdout/stderr lines and exit codes as the reference; the
 // computation is gpupi_b200's pipeline (pi_engine.cu).  --tuned (an addition)
 // shares forward transforms within each merge level instead of the
-// reference's op sequence; both print the same RET and digits.
+// reference's op sequence; both print the same RET and digits.  --output FILE
+// (an addition; default or --benchmark mode) writes "3<digits>\n" to FILE
+// instead of stdout.  Digits are streamed out after the timed region: each
+// chunk's device-to-host copy overlaps the write of the chunk before.
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -66,7 +69,8 @@ void hex_preview(const char *label, const uint32_t *limbs, uint32_t length) {   
 }
 
 void usage(const char *prog) {
-    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--tuned]\n", prog);
+    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE]\n",
+            prog);
 }
 
 }  // namespace
@@ -84,17 +88,27 @@ int main(int argc, char **argv) {
     }
     const uint32_t requested = (uint32_t)target;
     bool benchmark = false, profile = false, full = false, tuned = false;
+    const char *out_path = nullptr;
     int modes = 0;
     for (int i = 2; i < argc; ++i) {
         if (strcmp(argv[i], "--benchmark") == 0) benchmark = true, ++modes;
         else if (strcmp(argv[i], "--profile-stages") == 0) profile = true, ++modes;
         else if (strcmp(argv[i], "--full-print") == 0) full = true, ++modes;
         else if (strcmp(argv[i], "--tuned") == 0 && !tuned) tuned = true;
+        else if (strcmp(argv[i], "--output") == 0 && !out_path && i + 1 < argc) out_path = argv[++i];
         else modes = 2;
     }
-    if (modes > 1) {
+    if (modes > 1 || (out_path && (profile || full))) {
         usage(argv[0]);
         return 1;
+    }
+    FILE *out_file = nullptr;
+    if (out_path) {
+        out_file = fopen(out_path, "wb");
+        if (!out_file) {
+            fprintf(stderr, "cannot open %s\n", out_path);
+            return 1;
+        }
     }
     gpupi::PiRequest req;
     req.digits = requested;
@@ -102,12 +116,47 @@ int main(int argc, char **argv) {
     req.profile_stages = profile;
     if (benchmark) req.copy_digits = std::min<uint32_t>(requested, 63u);
     else if (profile) req.copy_digits = std::min<uint32_t>(requested, 4096u);
-    else req.copy_digits = requested;
+    else if (full) req.copy_digits = requested;
+    else req.copy_digits = 0u;   // streamed
     gpupi::PiOutput out;
+    // Streamed digits (after the timed region).  In the default mode the first
+    // chunk first prints the result line to stderr and "3" to stdout, the
+    // order in which the reference prints them; --output sends "3<digits>" to
+    // the file instead.
+    struct Sink {
+        FILE *f;
+        const gpupi::PiOutput *out;
+        uint32_t requested;
+        bool announce;
+        bool started;
+    } sink{out_file ? out_file : stdout, &out, requested, !out_file && !benchmark, false};
+    if (requested > 0u && (out_file || (!benchmark && !profile && !full))) {
+        req.sink = [](const char *data, size_t n, void *user) {
+            Sink *k = static_cast<Sink *>(user);
+            if (!k->started) {
+                if (k->announce)
+                    fprintf(stderr, "target_digits=%u convert_digits=%u RET_len=%u elapsed_ms=%.3f\n", k->requested,
+                            k->out->convert_digits, k->out->ret_len, k->out->elapsed_ms);
+                fputc('3', k->f);
+                k->started = true;
+            }
+            return fwrite(data, 1, n, k->f) == n;
+        };
+        req.sink_user = &sink;
+    }
     const cudaError_t err = gpupi::pi_run(req, out);
     if (err != cudaSuccess) {
         fprintf(stderr, "pi_fractional failed: %s\n", cudaGetErrorString(err));
+        if (out_file) fclose(out_file);
         return 1;
+    }
+    if (out_file) {
+        if (!sink.started) fputc('3', out_file);
+        fputc('\n', out_file);
+        const bool ok = fclose(out_file) == 0;
+        fprintf(stderr, "output=%s bytes=%llu output_ms=%.3f\n", out_path, (unsigned long long)requested + 2ull,
+                out.output_ms);
+        if (!ok) return 1;
     }
     const int ws_mb = (int)(out.workspace_bytes / (1024 * 1024));
     if (benchmark) {
@@ -156,8 +205,9 @@ int main(int argc, char **argv) {
             printf("DEC_preview_hash = %u\n", decimal_hash(out.digits.data(), (uint32_t)out.digits.size()));
         return 0;
     }
-    fprintf(stderr, "target_digits=%u convert_digits=%u RET_len=%u elapsed_ms=%.3f\n", requested,
-            out.convert_digits, out.ret_len, out.elapsed_ms);
+    if (!sink.started || !sink.announce)
+        fprintf(stderr, "target_digits=%u convert_digits=%u RET_len=%u elapsed_ms=%.3f\n", requested,
+                out.convert_digits, out.ret_len, out.elapsed_ms);
     if (full) {
         printf("RET = ");
         if (out.ret_len == 0) {
@@ -176,9 +226,10 @@ int main(int argc, char **argv) {
             fwrite(out.digits.data(), 1, requested, stdout);
             printf("\n");
         }
-    } else {
+    } else if (out_file) {
+        return 0;
+    } else if (!sink.started) {
         fputc('3', stdout);
-        if (requested > 0u) fwrite(out.digits.data(), 1, requested, stdout);
     }
     fputc('\n', stdout);
     return 0;

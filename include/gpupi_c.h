@@ -127,6 +127,18 @@ int gpupi_mp_mul_spectra(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t
                          uint32_t Lb, const uint32_t *D, uint32_t Ld, const uint32_t *E, uint32_t Le, uint32_t *C,
                          uint32_t Lc);
 
+/* Streamed digits: the same computation as gpupi_pi_compute, then the
+ * first `digits` decimal digits after "3." handed to sink in order, in chunks
+ * of at most `chunk` bytes (0: 64 MiB).  Each chunk's device-to-host copy
+ * overlaps the sink call for the chunk before (two pinned buffers); a nonzero
+ * return from sink stops the output.  info as for gpupi_pi_compute, with
+ * info[6] = host milliseconds of the output (float bits).  flags bit 2 =
+ * tuned form.  No counterpart in the reference, whose CLI copies all digits
+ * and then writes them. */
+typedef int (*gpupi_digit_sink)(const char *data, size_t n, void *user);
+int gpupi_pi_stream(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, gpupi_digit_sink sink, void *user,
+                    size_t chunk, uint32_t *info);
+
 /* Per-kernel timing: CUDA events around each launch on the current stream,
  * with the launch's algorithmic HBM bytes.  The report has one line per
  * kernel family: "name launches total_ms total_bytes", then one line per

@@ -62,6 +62,15 @@ def test_cli_exists(built):
     assert r.returncode == 1 and "Usage" in r.stderr
 
 
+@pytest.mark.parametrize("args", [["100", "--bogus"], ["100", "--benchmark", "--full-print"],
+                                  ["100", "--output"], ["100", "--full-print", "--output", "x.txt"],
+                                  ["100", "--tuned", "--tuned"], ["-5"]])
+def test_cli_rejects_bad_arguments(built, args):
+    """Usage errors exit 1 before any device work, as the reference's CLI does."""
+    r = subprocess.run([str(ROOT / "gpupi_b200" / "pi_bs_gpu"), *args], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stderr
+
+
 def test_no_cpu_fallback_without_gpu():
     """Compute entry points refuse to run without a CUDA device."""
     import torch

@@ -115,3 +115,45 @@ def test_pi_beyond_the_reference_ceiling(ctx):
     positions = sorted(rng.randrange(0, min(top, 1 << 30)) for _ in range(8))
     bad, unsure = g.bbp_spot_check(big.ret, positions)
     assert not bad and not unsure
+
+
+def test_streamed_digits(ctx, tmp_path):
+    """Streamed output (chunked device-to-host copies overlapping the writes):
+    the chunks concatenate to the digits, a False return stops, and the file
+    helper writes the CLI's "3<digits>\\n"."""
+    import gpupi_b200 as g
+    d = 100000
+    want = g.pi_compute(d, ctx).dec
+    chunks = []
+    g.pi_stream(d, chunks.append, ctx, chunk=4096)
+    assert len(chunks) == (d + 4095) // 4096
+    assert b"".join(chunks).decode() == want
+    first = []
+    g.pi_stream(d, lambda b: (first.append(b), False)[1], ctx, chunk=4096)
+    assert first == [want[:4096].encode()]
+    path = tmp_path / "pi.txt"
+    g.pi_to_file(d, path, ctx, chunk=10000)
+    assert path.read_text() == "3" + want + "\n"
+
+
+def test_cli_output_modes(tmp_path):
+    """The CLI streams its digits: default mode prints the result line on
+    stderr before "3<digits>" on stdout (as the reference orders them),
+    --output FILE writes the same bytes to a file, --full-print is unchanged."""
+    import subprocess
+    cli = str(Path(__file__).resolve().parents[1] / "gpupi_b200" / "pi_bs_gpu")
+    d = 100000
+    want = "3" + pi_ref.pi_digits(d).digits[:d] + "\n"
+    r = subprocess.run([cli, str(d)], capture_output=True, text=True, check=True)
+    assert r.stdout == want
+    assert r.stderr.startswith(f"target_digits={d} convert_digits=")
+    merged = subprocess.run([cli, str(d)], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                            check=True).stdout
+    assert merged.startswith(f"target_digits={d} ") and merged.endswith(want)
+    path = tmp_path / "pi.txt"
+    r = subprocess.run([cli, str(d), "--output", str(path)], capture_output=True, text=True, check=True)
+    assert r.stdout == "" and path.read_text() == want
+    assert f"output={path} bytes={d + 2}" in r.stderr
+    r = subprocess.run([cli, "1000", "--full-print"], capture_output=True, text=True, check=True)
+    # the DEC line, then the reference's closing newline (pi_bs_gpu.cu:2401-2423)
+    assert r.stdout.endswith("DEC = 3" + pi_ref.pi_digits(1000).digits[:1000] + "\n\n")
