@@ -69,6 +69,8 @@ _SIGS = [
     ("gpupi_mp_mul_ragged", ctypes.c_int, [_p, _u32, _p, _p, _p, _p, _p, _p, _p, _p]),
     ("gpupi_mp_mul_spectra", ctypes.c_int, [_p, _u32, _p, _u32, _p, _u32, _p, _u32, _p, _u32, _p, _u32]),
     ("gpupi_pi_stream", ctypes.c_int, [_p, _u32, _u32, _p, _p, ctypes.c_size_t, _p]),
+    ("gpupi_pi_compute_checkpointed", ctypes.c_int,
+     [_p, _u32, _u32, ctypes.c_char_p, _p, ctypes.c_size_t, _p, ctypes.c_size_t, _p]),
 ]
 
 _DIGIT_SINK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
@@ -343,7 +345,7 @@ def ret_limbs_bound(digits: int) -> int:
 
 def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None = None,
                ret_capacity: int | None = None, device_only: bool = False, profile: bool = False,
-               host_digits=None, host_ret=None, tuned: bool = False) -> PiResult:
+               host_digits=None, host_ret=None, tuned: bool = False, checkpoint=None) -> PiResult:
     """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional).
 
     ``host_digits`` / ``host_ret``: optional writable host buffers (e.g. pinned
@@ -352,7 +354,10 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
     the device.  ``device_only`` keeps RET and the digits on the device (no
     host copies at all).  ``tuned`` shares forward transforms within each
     merge level of the splitting tree instead of the reference's op sequence
-    (one batched product per op); both give the same RET and digits."""
+    (one batched product per op); both give the same RET and digits.
+    ``checkpoint``: a file for the splitting tree's result, loaded when valid
+    for this digit count (the tree is skipped) and written otherwise;
+    ``checkpoint_state`` on the result is 1 (loaded) or 2 (written)."""
     _torch()
     l = lib()
     if copy_digits is None:
@@ -372,14 +377,21 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
         dptr = ctypes.addressof(dbuf) if copy_digits else None
     info = (_u32 * 8)()
     flags = (1 if profile else 0) | (2 if device_only else 0) | (4 if tuned else 0)
-    rc = l.gpupi_pi_compute(ctx.h if ctx else None, digits, flags, ret.ctypes.data if ret_capacity else None,
-                            ret_capacity, dptr, copy_digits, info)
+    if checkpoint is not None:
+        rc = l.gpupi_pi_compute_checkpointed(ctx.h if ctx else None, digits, flags, str(checkpoint).encode(),
+                                             ret.ctypes.data if ret_capacity else None, ret_capacity, dptr,
+                                             copy_digits, info)
+    else:
+        rc = l.gpupi_pi_compute(ctx.h if ctx else None, digits, flags, ret.ctypes.data if ret_capacity else None,
+                                ret_capacity, dptr, copy_digits, info)
     _check(rc, "gpupi_pi_compute")
     ret_len = info[1]
     elapsed = np.frombuffer(np.uint32(info[2]).tobytes(), dtype=np.float32)[0]
     dec = dbuf.raw[:copy_digits].decode("ascii") if dbuf is not None else ""
-    return PiResult(digits, info[0], ret_len, float(elapsed), info[3],
-                    ret[:ret_len] if ret_capacity else None, dec, info[5])
+    r = PiResult(digits, info[0], ret_len, float(elapsed), info[3],
+                 ret[:ret_len] if ret_capacity else None, dec, info[5])
+    r.checkpoint_state = int(info[7]) if checkpoint is not None else 0
+    return r
 
 
 def pi_stream(digits: int, write, ctx: Context | None = None, chunk: int = 0, tuned: bool = False) -> PiResult:

@@ -239,6 +239,39 @@ int gpupi_pi_stream(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, gpupi_digit
     return 0;
 }
 
+int gpupi_pi_compute_checkpointed(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, const char *checkpoint,
+                                  uint32_t *h_ret, size_t ret_cap, char *h_digits, size_t digits_cap,
+                                  uint32_t *info) {
+    if (!checkpoint) return (int)cudaErrorInvalidValue;
+    gpupi::PiRequest req;
+    req.digits = digits;
+    req.profile_stages = (flags & 1u) != 0u;
+    req.copy_digits = h_digits ? (uint32_t)std::min<size_t>(digits_cap, digits) : 0u;
+    req.ctx = raw(ctx);
+    req.device_only = (flags & 2u) != 0u;
+    req.tuned = (flags & 4u) != 0u;
+    req.host_digits = h_digits;
+    req.host_ret = h_ret;
+    req.host_ret_cap = h_ret ? ret_cap : 0;
+    req.checkpoint = checkpoint;
+    gpupi::PiOutput out;
+    cudaError_t err = gpupi::pi_run(req, out);
+    if (err != cudaSuccess) return (int)err;
+    if (info) {
+        uint32_t leaf = 0u;
+        gpupi::round_up_decimal_digits(digits, &leaf);
+        info[0] = out.convert_digits;
+        info[1] = out.ret_len;
+        memcpy(&info[2], &out.elapsed_ms, 4);
+        info[3] = (uint32_t)(out.workspace_bytes >> 20);
+        info[4] = (uint32_t)out.stages.size();
+        info[5] = leaf;
+        info[6] = 0u;
+        info[7] = (uint32_t)out.checkpoint;
+    }
+    return 0;
+}
+
 int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
                      char *h_digits, size_t digits_cap, uint32_t *info) {
     gpupi::PiRequest req;

@@ -36,6 +36,10 @@ struct PiRequest {
     bool (*sink)(const char *data, size_t n, void *user) = nullptr;
     void *sink_user = nullptr;
     size_t sink_chunk = (size_t)64 << 20;
+    // Checkpoint file of the splitting tree's result: loaded (and the tree
+    // skipped) when it holds a valid result for this digit count's tree,
+    // else written after the tree.  Null: none.
+    const char *checkpoint = nullptr;
 };
 
 struct PiOutput {
@@ -44,6 +48,7 @@ struct PiOutput {
     uint32_t ret_len = 0;
     float elapsed_ms = 0.f;
     float output_ms = 0.f;          // host time of the streamed output (sink set)
+    int checkpoint = 0;             // 1: tree loaded from the checkpoint, 2: tree computed and saved
     size_t workspace_bytes = 0;
     std::vector<uint32_t> ret;      // RET limbs (little endian)
     std::string digits;             // first copy_digits digits (unless PiRequest::host_digits)

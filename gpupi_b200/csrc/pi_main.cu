@@ -1,6 +1,7 @@
 // pi_bs_gpu command line (gpupi pi_bs_gpu.cu:2073-2437, main_fractional).
 //
 //   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE]
+//             [--checkpoint FILE]
 //
 // Same arguments, stdout/stderr lines and exit codes as the reference; the
 // computation is gpupi_b200's pipeline (pi_engine.cu).  --tuned (an addition)
@@ -9,6 +10,8 @@
 // (an addition; default or --benchmark mode) writes "3<digits>\n" to FILE
 // instead of stdout.  Digits are streamed out after the timed region: each
 // chunk's device-to-host copy overlaps the write of the chunk before.
+// --checkpoint FILE (an addition) loads the splitting tree's result from
+// FILE when it is valid for this digit count and otherwise writes it there.
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -69,7 +72,8 @@ void hex_preview(const char *label, const uint32_t *limbs, uint32_t length) {   
 }
 
 void usage(const char *prog) {
-    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE]\n",
+    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE] "
+            "[--checkpoint FILE]\n",
             prog);
 }
 
@@ -88,7 +92,7 @@ int main(int argc, char **argv) {
     }
     const uint32_t requested = (uint32_t)target;
     bool benchmark = false, profile = false, full = false, tuned = false;
-    const char *out_path = nullptr;
+    const char *out_path = nullptr, *ckpt_path = nullptr;
     int modes = 0;
     for (int i = 2; i < argc; ++i) {
         if (strcmp(argv[i], "--benchmark") == 0) benchmark = true, ++modes;
@@ -96,6 +100,7 @@ int main(int argc, char **argv) {
         else if (strcmp(argv[i], "--full-print") == 0) full = true, ++modes;
         else if (strcmp(argv[i], "--tuned") == 0 && !tuned) tuned = true;
         else if (strcmp(argv[i], "--output") == 0 && !out_path && i + 1 < argc) out_path = argv[++i];
+        else if (strcmp(argv[i], "--checkpoint") == 0 && !ckpt_path && i + 1 < argc) ckpt_path = argv[++i];
         else modes = 2;
     }
     if (modes > 1 || (out_path && (profile || full))) {
@@ -114,6 +119,7 @@ int main(int argc, char **argv) {
     req.digits = requested;
     req.tuned = tuned;
     req.profile_stages = profile;
+    req.checkpoint = ckpt_path;
     if (benchmark) req.copy_digits = std::min<uint32_t>(requested, 63u);
     else if (profile) req.copy_digits = std::min<uint32_t>(requested, 4096u);
     else if (full) req.copy_digits = requested;
@@ -150,6 +156,8 @@ int main(int argc, char **argv) {
         if (out_file) fclose(out_file);
         return 1;
     }
+    if (ckpt_path)
+        fprintf(stderr, "checkpoint=%s %s\n", ckpt_path, out.checkpoint == 1 ? "loaded" : "written");
     if (out_file) {
         if (!sink.started) fputc('3', out_file);
         fputc('\n', out_file);

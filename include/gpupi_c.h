@@ -127,6 +127,16 @@ int gpupi_mp_mul_spectra(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t
                          uint32_t Lb, const uint32_t *D, uint32_t Ld, const uint32_t *E, uint32_t Le, uint32_t *C,
                          uint32_t Lc);
 
+/* gpupi_pi_compute with a checkpoint file of the splitting tree's result
+ * (Q and R, about 1 GB at 1e9 digits): when the file holds a valid result for
+ * this digit count's tree (header, tree size and checksum match) it is loaded
+ * and the tree is skipped, else the tree runs and the file is written
+ * (through a temporary name, renamed when complete).  info[7] = 1 loaded,
+ * 2 written.  No counterpart in the reference. */
+int gpupi_pi_compute_checkpointed(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, const char *checkpoint,
+                                  uint32_t *h_ret, size_t ret_cap, char *h_digits, size_t digits_cap,
+                                  uint32_t *info);
+
 /* Streamed digits: the same computation as gpupi_pi_compute, then the
  * first `digits` decimal digits after "3." handed to sink in order, in chunks
  * of at most `chunk` bytes (0: 64 MiB).  Each chunk's device-to-host copy

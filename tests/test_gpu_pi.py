@@ -157,3 +157,39 @@ def test_cli_output_modes(tmp_path):
     r = subprocess.run([cli, "1000", "--full-print"], capture_output=True, text=True, check=True)
     # the DEC line, then the reference's closing newline (pi_bs_gpu.cu:2401-2423)
     assert r.stdout.endswith("DEC = 3" + pi_ref.pi_digits(1000).digits[:1000] + "\n\n")
+
+
+def test_checkpoint_of_the_tree(ctx, tmp_path):
+    """The splitting tree's result saved to a checkpoint and loaded back gives
+    the same RET and digits; a corrupted, truncated or other-size checkpoint
+    is not used (the tree runs and the file is rewritten)."""
+    import gpupi_b200 as g
+    d = 300_000
+    want = g.pi_compute(d, ctx)
+    ck = tmp_path / "tree.ckpt"
+    a = g.pi_compute(d, ctx, checkpoint=ck)
+    assert a.checkpoint_state == 2 and ck.exists()
+    b = g.pi_compute(d, ctx, checkpoint=ck)
+    assert b.checkpoint_state == 1
+    for r in (a, b):
+        assert np.array_equal(r.ret, want.ret) and r.dec == want.dec
+    raw = bytearray(ck.read_bytes())
+    raw[len(raw) // 2] ^= 1
+    ck.write_bytes(bytes(raw))
+    c = g.pi_compute(d, ctx, checkpoint=ck)
+    assert c.checkpoint_state == 2 and c.dec == want.dec
+    assert g.pi_compute(d, ctx, checkpoint=ck).checkpoint_state == 1
+    ck.write_bytes(ck.read_bytes()[:-4])
+    assert g.pi_compute(d, ctx, checkpoint=ck).checkpoint_state == 2
+    small = g.pi_compute(20_000, ctx, checkpoint=ck)   # another tree size
+    assert small.checkpoint_state == 2 and small.dec == g.pi_compute(20_000, ctx).dec
+
+
+def test_cli_checkpoint(tmp_path):
+    import subprocess
+    cli = str(Path(__file__).resolve().parents[1] / "gpupi_b200" / "pi_bs_gpu")
+    ck = tmp_path / "tree.ckpt"
+    r1 = subprocess.run([cli, "100000", "--checkpoint", str(ck)], capture_output=True, text=True, check=True)
+    r2 = subprocess.run([cli, "100000", "--checkpoint", str(ck)], capture_output=True, text=True, check=True)
+    assert f"checkpoint={ck} written" in r1.stderr and f"checkpoint={ck} loaded" in r2.stderr
+    assert r1.stdout == r2.stdout == "3" + pi_ref.pi_digits(100000).digits[:100000] + "\n"
