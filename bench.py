@@ -268,20 +268,20 @@ def run_ours(args, ws, rank, local):
     ms_local = e0.elapsed_time(e1) / args.steps
     ms = _max_over_ranks(ms_local, ws)
 
-    # the tuned form (forward transforms shared within merge levels; same
-    # RET and digits), device-timed the same way
+    # the plain form (the reference's op sequence; same RET and digits),
+    # device-timed the same way
     for _ in range(max(1, args.warmup - 1)):
-        g.pi_compute(digits, ctx, device_only=True, tuned=True)
+        g.pi_compute(digits, ctx, device_only=True, plain=True)
     _barrier(ws)
     torch.cuda.synchronize()
     e4 = torch.cuda.Event(enable_timing=True)
     e5 = torch.cuda.Event(enable_timing=True)
     e4.record()
     for _ in range(args.steps):
-        rt = g.pi_compute(digits, ctx, device_only=True, tuned=True)
+        rp = g.pi_compute(digits, ctx, device_only=True, plain=True)
     e5.record()
     torch.cuda.synchronize()
-    ms_tuned = _max_over_ranks(e4.elapsed_time(e5) / args.steps, ws)
+    ms_plain = _max_over_ranks(e4.elapsed_time(e5) / args.steps, ws)
 
     # the same steps again with per-launch CUDA events around every kernel
     # (kernel families and the roofline of the dominant one)
@@ -364,11 +364,12 @@ def run_ours(args, ws, rank, local):
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (pi has no input data)",
         "config": {"workload": f"pi to {digits} decimal digits (pi_bs_gpu {digits})", "digits": digits,
-                   "form": "plain (one op per launch, compact after every op, reference op sequence)",
+                   "form": "tuned (forward transforms shared within each merge level of the splitting tree; "
+                           "otherwise the reference's op sequence, one op per launch, compact after every op)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "working set (tens of GB) larger than L2; no flush needed"},
-        "forms": {"plain_ms": ms, "tuned_ms": ms_tuned, "plain_over_tuned": ms / ms_tuned,
-                  "tuned_ret_len": rt.ret_len},
+        "forms": {"tuned_ms": ms, "plain_ms": ms_plain, "plain_over_tuned": ms_plain / ms,
+                  "plain_ret_len": rp.ret_len},
         "pipeline_elapsed_ms": statistics.mean(inner),
         "step_ms": [round(x, 3) for x in inner],
         "ms_per_step_with_kernel_timers": ms_timed_local,

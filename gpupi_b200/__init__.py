@@ -345,16 +345,17 @@ def ret_limbs_bound(digits: int) -> int:
 
 def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None = None,
                ret_capacity: int | None = None, device_only: bool = False, profile: bool = False,
-               host_digits=None, host_ret=None, tuned: bool = False, checkpoint=None) -> PiResult:
+               host_digits=None, host_ret=None, plain: bool = False, checkpoint=None) -> PiResult:
     """Run pi_bs_gpu's pipeline for ``digits`` digits (pi_bs_gpu.cu main_fractional).
 
     ``host_digits`` / ``host_ret``: optional writable host buffers (e.g. pinned
     torch tensors: uint8 for the digits, 32-bit for RET, at least
     ret_limbs_bound(digits) limbs) receiving the digits and RET directly from
     the device.  ``device_only`` keeps RET and the digits on the device (no
-    host copies at all).  ``tuned`` shares forward transforms within each
-    merge level of the splitting tree instead of the reference's op sequence
-    (one batched product per op); both give the same RET and digits.
+    host copies at all).  ``plain`` runs the reference's op sequence (one
+    batched product per op) instead of the default tuned form, which shares
+    forward transforms within each merge level of the splitting tree; both
+    give the same RET and digits.
     ``checkpoint``: a file for the splitting tree's result, loaded when valid
     for this digit count (the tree is skipped) and written otherwise;
     ``checkpoint_state`` on the result is 1 (loaded) or 2 (written)."""
@@ -376,7 +377,7 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
         dbuf = ctypes.create_string_buffer(max(copy_digits, 1))
         dptr = ctypes.addressof(dbuf) if copy_digits else None
     info = (_u32 * 8)()
-    flags = (1 if profile else 0) | (2 if device_only else 0) | (4 if tuned else 0)
+    flags = (1 if profile else 0) | (2 if device_only else 0) | (4 if plain else 0)
     if checkpoint is not None:
         rc = l.gpupi_pi_compute_checkpointed(ctx.h if ctx else None, digits, flags, str(checkpoint).encode(),
                                              ret.ctypes.data if ret_capacity else None, ret_capacity, dptr,
@@ -394,7 +395,7 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
     return r
 
 
-def pi_stream(digits: int, write, ctx: Context | None = None, chunk: int = 0, tuned: bool = False) -> PiResult:
+def pi_stream(digits: int, write, ctx: Context | None = None, chunk: int = 0, plain: bool = False) -> PiResult:
     """Compute pi to ``digits`` digits and pass the digits after "3." to
     ``write(bytes)`` in order, in chunks of at most ``chunk`` bytes (0: 64 MiB),
     each chunk's device-to-host copy overlapping the previous write
@@ -413,7 +414,7 @@ def pi_stream(digits: int, write, ctx: Context | None = None, chunk: int = 0, tu
 
     cb = _DIGIT_SINK(_sink)
     info = (_u32 * 8)()
-    rc = lib().gpupi_pi_stream(ctx.h if ctx else None, digits, 4 if tuned else 0,
+    rc = lib().gpupi_pi_stream(ctx.h if ctx else None, digits, 4 if plain else 0,
                                ctypes.cast(cb, ctypes.c_void_p), None, chunk, info)
     if failed:
         raise failed[0]
@@ -424,11 +425,11 @@ def pi_stream(digits: int, write, ctx: Context | None = None, chunk: int = 0, tu
     return r
 
 
-def pi_to_file(digits: int, path, ctx: Context | None = None, chunk: int = 0, tuned: bool = False) -> PiResult:
+def pi_to_file(digits: int, path, ctx: Context | None = None, chunk: int = 0, plain: bool = False) -> PiResult:
     """Write "3<digits>\\n" to ``path`` (the CLI's output), streamed."""
     with open(path, "wb") as f:
         f.write(b"3")
-        r = pi_stream(digits, f.write, ctx, chunk, tuned)
+        r = pi_stream(digits, f.write, ctx, chunk, plain)
         f.write(b"\n")
     return r
 

@@ -214,7 +214,7 @@ int gpupi_pi_stream(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, gpupi_digit
     gpupi::PiRequest req;
     req.digits = digits;
     req.ctx = raw(ctx);
-    req.tuned = (flags & 4u) != 0u;
+    req.plain = (flags & 4u) != 0u;
     req.sink = [](const char *data, size_t n, void *u) {
         StreamSink *s = static_cast<StreamSink *>(u);
         return s->fn(data, n, s->user) == 0;
@@ -249,7 +249,7 @@ int gpupi_pi_compute_checkpointed(gpupi_ctx *ctx, uint32_t digits, uint32_t flag
     req.copy_digits = h_digits ? (uint32_t)std::min<size_t>(digits_cap, digits) : 0u;
     req.ctx = raw(ctx);
     req.device_only = (flags & 2u) != 0u;
-    req.tuned = (flags & 4u) != 0u;
+    req.plain = (flags & 4u) != 0u;
     req.host_digits = h_digits;
     req.host_ret = h_ret;
     req.host_ret_cap = h_ret ? ret_cap : 0;
@@ -280,7 +280,7 @@ int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *
     req.copy_digits = h_digits ? (uint32_t)std::min<size_t>(digits_cap, digits) : 0u;
     req.ctx = raw(ctx);
     req.device_only = (flags & 2u) != 0u;
-    req.tuned = (flags & 4u) != 0u;
+    req.plain = (flags & 4u) != 0u;
     req.host_digits = h_digits;
     req.host_ret = h_ret;
     req.host_ret_cap = h_ret ? ret_cap : 0;

@@ -469,11 +469,13 @@ __global__ void __launch_bounds__(128) k_rows_small(NttParams P, RowsArgs a) {
 // Split row passes for products that share forward transforms.
 //
 // k_rows_fwd finishes the forward transform of one or two operands whose
-// column passes are done and stores each row segment in the thread order of
-// its last stage (thread t holds positions 16t .. 16t + 15: four 16-byte
-// stores).  k_rows_inv reads T pairs of such spectra in the same order,
-// forms sum_t X_t Y_t K^-1 (mod p) and runs the inverse stages, leaving the
-// segment in the order the inverse column passes expect, exactly as the
+// column passes are done; the last stage's registers (thread t holds
+// positions 16t .. 16t + 15) go through the shared tile to the first
+// stage's order (thread t holds t + 256 j), so the spectrum is stored with
+// coalesced 128-byte warp accesses.  k_rows_inv loads T pairs of spectra in
+// that order, forms sum_t X_t Y_t K^-1 (mod p), moves the result back to
+// the last stage's order through the tile and runs the inverse stages,
+// leaving the segment in the order the inverse column passes expect, as the
 // fused k_rows_r does.  So a transform computed once serves every product
 // it takes part in, and a sum of products costs one inverse transform.
 // ---------------------------------------------------------------------------
@@ -505,11 +507,17 @@ __device__ __forceinline__ void rows_fwd_body(const RowsFwdArgs &a, uint64_t b, 
             First::elem(t, j, pos, c);
             x[j] = F[pos];
         }
-        __syncthreads();   // twiddles loaded; the previous operand's last stage has left the tile
+        __syncthreads();   // twiddles loaded; the previous operand has left the tile
         run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
-        uint4 *out = reinterpret_cast<uint4 *>(F + 16u * t);
+        SplitLast::store(Sm, x, t);   // every thread passed the last stage's tile loads
+        __syncthreads();
 #pragma unroll
-        for (int v = 0; v < 4; ++v) out[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            F[pos] = Sm[First::addr(pos, c)];
+        }
+        __syncthreads();
     }
     (void)T;
 }
@@ -549,25 +557,26 @@ __device__ __forceinline__ void rows_inv_body(const NttParams &P, const RowsInvA
     const uint64_t off = (b / nseg) * 3 * K + (uint64_t)Q * K + ((uint64_t)(b % nseg) << kSplitLogC);
     const uint32_t t = threadIdx.x;
     const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + Q);
+    using First = typename ExecStage<kSplitLogC, 0, false, 0>::S;
     uint32_t x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) x[j] = 0u;
 #pragma unroll
     for (int term = 0; term < TERMS; ++term) {
-        const uint4 *X = reinterpret_cast<const uint4 *>(a.X[term] + off + 16u * t);
-        const uint4 *Y = reinterpret_cast<const uint4 *>(a.Y[term] + off + 16u * t);
+        const uint32_t *X = a.X[term] + off, *Y = a.Y[term] + off;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const uint4 u = X[v], w = Y[v];
-            x[4 * v] = add_n<Q>(x[4 * v], norm<Q>(mont<Q>(u.x, w.x)));
-            x[4 * v + 1] = add_n<Q>(x[4 * v + 1], norm<Q>(mont<Q>(u.y, w.y)));
-            x[4 * v + 2] = add_n<Q>(x[4 * v + 2], norm<Q>(mont<Q>(u.z, w.z)));
-            x[4 * v + 3] = add_n<Q>(x[4 * v + 3], norm<Q>(mont<Q>(u.w, w.w)));
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            x[j] = add_n<Q>(x[j], norm<Q>(mont<Q>(__ldg(X + pos), __ldg(Y + pos))));
         }
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(x[j], scale));   // sum K^-1
-    __syncthreads();   // inverse twiddles loaded
+    First::store(Sm, x, t);
+    __syncthreads();   // tile written, inverse twiddles loaded
+    SplitLast::load(Sm, x, t);
+    __syncthreads();
     run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {

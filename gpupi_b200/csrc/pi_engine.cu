@@ -296,11 +296,15 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
         });
     };
     // P' = P_e P_o (P_e kept for R2)
+    // P_e and P_o share one launch per pass for the pb rows they both have;
+    // when P has an odd row count (pb = half - 1) P_e's last row follows alone
     TRY(stage(pr, "fwd", "P_e,P_o", n1, half, lp, lp, true, [&]() {
         TRY(fpe.alloc(words));
         TRY(fpo.alloc(words));
-        spectrum_forward(tab, S, half, P_even.data, P_even.stride, lp, fpe.p, nullptr, 0, 0, nullptr);
-        spectrum_forward(tab, S, pb, P_odd.data, P_odd.stride, lp, fpo.p, nullptr, 0, 0, nullptr);
+        spectrum_forward(tab, S, pb, P_even.data, P_even.stride, lp, fpe.p, P_odd.data, P_odd.stride, lp, fpo.p);
+        if (pb < half)
+            spectrum_forward(tab, S, 1u, P_even.data + (size_t)pb * P_even.stride, P_even.stride, lp,
+                             fpe.p + spectrum_words(S, pb), nullptr, 0, 0, nullptr);
         return cudaGetLastError();
     }));
     Pn = BatchMPArray{nullptr, 2u * lp, pb, 2u * lp};
@@ -985,18 +989,20 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     cudaError_t err = cudaEventRecord(e0, st);
     // Size the multiply workspace once for the largest product (P * invQ, two
     // operands of about prec_limbs limbs) so that no level regrows it, and
-    // the scratch arena for every level's temporaries (at most about 16
-    // bytes per digit at 3e8 and 1e9 digits; the margin absorbs
-    // fragmentation, and a request that still misses spills to the pool).
+    // the scratch arena for every level's temporaries (high-water marks of
+    // 16 B per digit for the plain form and up to 32 B per digit for the
+    // tuned form's spectra, at 3e8 digits; the margin absorbs fragmentation,
+    // and a request that still misses spills to the pool).
     if (err == cudaSuccess)
         err = batch_mp_ensure_workspace(ctx, batch_mul_ntt_workspace_size(1u, prec + 8u, prec + 8u));
-    if (err == cudaSuccess) scratch_reserve((size_t)requested * 21u + (16u << 20));
+    if (err == cudaSuccess)
+        scratch_reserve((size_t)requested * (req.plain ? 21u : 40u) + ((size_t)64 << 20));
     Buf retb;
     BatchMPArray RET{};
     ConvertDecimalPowerTable powers{};
     char *d_digits = nullptr;
     if (err == cudaSuccess)
-        err = pi_fractional(ctx, &prof, (int)requested, retb, RET, req.tuned, req.checkpoint, &out.checkpoint);
+        err = pi_fractional(ctx, &prof, (int)requested, retb, RET, !req.plain, req.checkpoint, &out.checkpoint);
     // RET into the caller's buffer on a side stream, overlapping the decimal
     // conversion (which only reads RET)
     cudaStream_t side = nullptr;

@@ -28,7 +28,7 @@ struct PiRequest {
     char *host_digits = nullptr;    // caller buffer (>= copy_digits bytes, may be pinned) for the digits
     uint32_t *host_ret = nullptr;   // caller buffer for RET (copied while the digits are converted)
     size_t host_ret_cap = 0;        // its capacity in limbs
-    bool tuned = false;             // share forward transforms within merge levels (same results)
+    bool plain = false;             // the reference's op sequence; default: shared forward transforms (same results)
     // Streamed digit output: after the timed region the requested digits are
     // handed to sink in order, in chunks of at most sink_chunk bytes; each
     // chunk's device-to-host copy (two pinned buffers, one copy stream)

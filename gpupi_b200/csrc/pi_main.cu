@@ -1,12 +1,14 @@
 // pi_bs_gpu command line (gpupi pi_bs_gpu.cu:2073-2437, main_fractional).
 //
-//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE]
+//   pi_bs_gpu <digits> [--benchmark|--profile-stages|--full-print] [--plain] [--output FILE]
 //             [--checkpoint FILE]
 //
 // Same arguments, stdout/stderr lines and exit codes as the reference; the
-// computation is gpupi_b200's pipeline (pi_engine.cu).  --tuned (an addition)
-// shares forward transforms within each merge level instead of the
-// reference's op sequence; both print the same RET and digits.  --output FILE
+// computation is gpupi_b200's pipeline (pi_engine.cu), by default in its
+// tuned form (forward transforms shared within each merge level of the
+// splitting tree); --plain (an addition) runs the reference's op sequence,
+// which --profile-stages also uses so that its stage list is the
+// reference's.  Both print the same RET and digits.  --output FILE
 // (an addition; default or --benchmark mode) writes "3<digits>\n" to FILE
 // instead of stdout.  Digits are streamed out after the timed region: each
 // chunk's device-to-host copy overlaps the write of the chunk before.
@@ -72,7 +74,7 @@ void hex_preview(const char *label, const uint32_t *limbs, uint32_t length) {   
 }
 
 void usage(const char *prog) {
-    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--tuned] [--output FILE] "
+    fprintf(stderr, "Usage: %s <target_digits> [--benchmark|--profile-stages|--full-print] [--plain] [--output FILE] "
             "[--checkpoint FILE]\n",
             prog);
 }
@@ -91,14 +93,14 @@ int main(int argc, char **argv) {
         return 1;
     }
     const uint32_t requested = (uint32_t)target;
-    bool benchmark = false, profile = false, full = false, tuned = false;
+    bool benchmark = false, profile = false, full = false, plain = false;
     const char *out_path = nullptr, *ckpt_path = nullptr;
     int modes = 0;
     for (int i = 2; i < argc; ++i) {
         if (strcmp(argv[i], "--benchmark") == 0) benchmark = true, ++modes;
         else if (strcmp(argv[i], "--profile-stages") == 0) profile = true, ++modes;
         else if (strcmp(argv[i], "--full-print") == 0) full = true, ++modes;
-        else if (strcmp(argv[i], "--tuned") == 0 && !tuned) tuned = true;
+        else if (strcmp(argv[i], "--plain") == 0 && !plain) plain = true;
         else if (strcmp(argv[i], "--output") == 0 && !out_path && i + 1 < argc) out_path = argv[++i];
         else if (strcmp(argv[i], "--checkpoint") == 0 && !ckpt_path && i + 1 < argc) ckpt_path = argv[++i];
         else modes = 2;
@@ -117,7 +119,8 @@ int main(int argc, char **argv) {
     }
     gpupi::PiRequest req;
     req.digits = requested;
-    req.tuned = tuned;
+    // --profile-stages lists the reference's stages: it runs the plain form
+    req.plain = plain || profile;
     req.profile_stages = profile;
     req.checkpoint = ckpt_path;
     if (benchmark) req.copy_digits = std::min<uint32_t>(requested, 63u);

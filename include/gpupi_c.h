@@ -107,11 +107,10 @@ int gpupi_convert_decimal(gpupi_ctx *ctx, const uint32_t *d_X, uint32_t L_x, uin
  * may be null.  info[0..7] receives: convert_digits, RET length, elapsed ms
  * on the device (float bits), workspace MB, number of profiled stages, leaf
  * digits, 0, 0.  flags bit 0 = profile every stage, bit 1 = keep RET and the
- * digits on the device (no host copies), bit 2 = tuned form: forward
- * transforms shared within each merge level of the splitting tree and R'
- * summed in the transform domain (the default is the reference's op
- * sequence, one batched product per op; both give the same RET and
- * digits). */
+ * digits on the device (no host copies), bit 2 = plain form: the
+ * reference's op sequence, one batched product per op (the default, tuned
+ * form shares forward transforms within each merge level of the splitting
+ * tree; both give the same RET and digits). */
 int gpupi_pi_compute(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, uint32_t *h_ret, size_t ret_cap,
                      char *h_digits, size_t digits_cap, uint32_t *info);
 
@@ -143,7 +142,7 @@ int gpupi_pi_compute_checkpointed(gpupi_ctx *ctx, uint32_t digits, uint32_t flag
  * overlaps the sink call for the chunk before (two pinned buffers); a nonzero
  * return from sink stops the output.  info as for gpupi_pi_compute, with
  * info[6] = host milliseconds of the output (float bits).  flags bit 2 =
- * tuned form.  No counterpart in the reference, whose CLI copies all digits
+ * plain form.  No counterpart in the reference, whose CLI copies all digits
  * and then writes them. */
 typedef int (*gpupi_digit_sink)(const char *data, size_t n, void *user);
 int gpupi_pi_stream(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, gpupi_digit_sink sink, void *user,

@@ -64,7 +64,7 @@ def test_cli_exists(built):
 
 @pytest.mark.parametrize("args", [["100", "--bogus"], ["100", "--benchmark", "--full-print"],
                                   ["100", "--output"], ["100", "--full-print", "--output", "x.txt"],
-                                  ["100", "--tuned", "--tuned"], ["-5"], ["100", "--checkpoint"]])
+                                  ["100", "--plain", "--plain"], ["-5"], ["100", "--checkpoint"]])
 def test_cli_rejects_bad_arguments(built, args):
     """Usage errors exit 1 before any device work, as the reference's CLI does."""
     r = subprocess.run([str(ROOT / "gpupi_b200" / "pi_bs_gpu"), *args], capture_output=True, text=True)

@@ -88,11 +88,11 @@ def test_scratch_arena_reaches_steady_state(ctx):
 @pytest.mark.parametrize("digits", [20000, 300000, 3000000])
 def test_plain_and_tuned_forms_agree(ctx, digits):
     """The plain form (the reference's op sequence) and the default tuned form
-    (forward transforms shared within each merge level, R' summed in the
-    transform domain) produce the same RET and digits."""
+    (forward transforms shared within each merge level) produce the same RET
+    and digits."""
     import gpupi_b200 as g
-    tuned = g.pi_compute(digits, ctx, tuned=True)
-    plain = g.pi_compute(digits, ctx)
+    tuned = g.pi_compute(digits, ctx)
+    plain = g.pi_compute(digits, ctx, plain=True)
     assert tuned.ret_len == plain.ret_len
     assert np.array_equal(tuned.ret, plain.ret)
     assert tuned.dec == plain.dec
