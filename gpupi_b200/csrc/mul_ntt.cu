@@ -596,12 +596,17 @@ __global__ void __launch_bounds__((1 << kSplitLogC) / 16, 4) k_rows_inv(NttParam
     const int q = grid_prime(b);
     const uint2 *lev = level_ptr(P.tab, 1, q);
     for (uint32_t e = threadIdx.x; e < C - 1; e += C / 16) tw[e] = __ldg(lev + e);
-    if (q == 0)
-        rows_inv_body<TERMS, 0>(P, a, b, Sm, tw);
-    else if (q == 1)
-        rows_inv_body<TERMS, 1>(P, a, b, Sm, tw);
-    else
-        rows_inv_body<TERMS, 2>(P, a, b, Sm, tw);
+    // two segments per CTA (their count is even: K >= 8192) share the
+    // twiddle table load
+    for (uint64_t s = 2 * b; s < 2 * b + 2; ++s) {
+        if (q == 0)
+            rows_inv_body<TERMS, 0>(P, a, s, Sm, tw);
+        else if (q == 1)
+            rows_inv_body<TERMS, 1>(P, a, s, Sm, tw);
+        else
+            rows_inv_body<TERMS, 2>(P, a, s, Sm, tw);
+        __syncthreads();   // the tile is free for the next segment
+    }
 }
 
 // Coset recombination.  Row r holds z_i[j] = C_i[j] g^(ij) for cosets i < M;
@@ -1142,7 +1147,7 @@ static void spectrum_inverse(const NttParams &P, Shape s, uint32_t N, int terms,
     r.Fout = Fout;
     r.terms = terms;
     r.log_k = log_k;
-    const unsigned blocks = (unsigned)(VR * kPrimes * (K >> kSplitLogC));
+    const unsigned blocks = (unsigned)(VR * kPrimes * (K >> kSplitLogC) / 2);   // two segments per CTA
     {
         KernelTimed kt("ntt_rows_inv", 4.0 * (double)K * (double)VR * kPrimes * (2.0 * terms + 1.0));
         if (terms == 1)
