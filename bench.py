@@ -42,9 +42,15 @@ ROOT = Path(__file__).resolve().parent
 # algorithmic bytes; part of the output is still in L2 at kernel end).  The
 # pi run's launches are scaled by their algorithmic bytes.
 BBP_POSITIONS = 64
-NCU_TRAFFIC_RATIO = {"ntt_rows_fused": 264.006 / 301.990}
-NCU_TRAFFIC_SOURCE = ("ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product, "
-                      "scaled to each launch by its algorithmic bytes")
+# DRAM bytes (read + write) over algorithmic bytes of one launch, from ncu
+# captures on 2^22 x 2^22-limb products (profiles/ntt_rows_cols_4Mi.md,
+# profiles/ntt_split_rows_4Mi.md); applied to each launch of the family
+NCU_TRAFFIC_RATIO = {"ntt_rows_fused": 264.006 / 301.990,
+                     "ntt_cols_fwd_first": 229.642496 / 234.881024}
+NCU_TRAFFIC_SOURCE = {"ntt_rows_fused": "ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product, "
+                                        "scaled to each launch by its algorithmic bytes",
+                      "ntt_cols_fwd_first": "ncu capture of k_cols_r<6, first, fwd, pair> on a 2^22 x 2^22-limb "
+                                            "product, scaled to each launch by its algorithmic bytes"}
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ms to 1e9 digits of pi (bit-exact), tuned vs plain form on B200; NTT HBM GB/s"
@@ -350,7 +356,7 @@ def run_ours(args, ws, rank, local):
                 "frac": achieved / peaks["hbm_gbs"],
                 "traffic": (ratio * kbytes / n) if ratio else None,
                 "traffic_unit": "bytes per launch (DRAM read + write)",
-                "traffic_source": NCU_TRAFFIC_SOURCE if ratio else None,
+                "traffic_source": NCU_TRAFFIC_SOURCE.get(name),
                 "launches_per_step": n / args.steps, "share_of_kernel_time": kms / total_kernel_ms,
                 "peak_source": "measured" if not peaks.get("fallback") else "fallback"}
     families = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
@@ -406,8 +412,15 @@ def run_ntt(args, ws, rank, local):
     A = torch.randint(-2 ** 31, 2 ** 31 - 1, (L,), dtype=torch.int32, device="cuda", generator=gen)
     B = torch.randint(-2 ** 31, 2 ** 31 - 1, (L,), dtype=torch.int32, device="cuda", generator=gen)
     C = torch.zeros(2 * L, dtype=torch.int32, device="cuda")
+
+    def step():
+        if args.ntt_path == "spectra":   # split row passes (the tuned form's building block)
+            ctx.mul_spectra(1, A.data_ptr(), L, B.data_ptr(), L, C.data_ptr(), 2 * L)
+        else:
+            ctx.mul(1, A.data_ptr(), L, L, B.data_ptr(), L, L, C.data_ptr(), 2 * L, 2 * L)
+
     for _ in range(args.warmup):
-        ctx.mul(1, A.data_ptr(), L, L, B.data_ptr(), L, L, C.data_ptr(), 2 * L, 2 * L)
+        step()
     torch.cuda.synchronize()
     g.timer_reset()
     g.timer_enable(True)
@@ -415,7 +428,7 @@ def run_ntt(args, ws, rank, local):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        ctx.mul(1, A.data_ptr(), L, L, B.data_ptr(), L, L, C.data_ptr(), 2 * L, 2 * L)
+        step()
     e1.record()
     torch.cuda.synchronize()
     g.timer_enable(False)
@@ -423,7 +436,7 @@ def run_ntt(args, ws, rank, local):
     fam = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
                "GBps": v[2] / (v[1] * 1e-3) / 1e9 if v[1] > 0 else None} for k, v in g.timer_report().items()}
     if rank == 0:
-        print(json.dumps({"metric": f"ms per {L}x{L}-limb NTT product", "value": ms, "unit": "ms",
+        print(json.dumps({"metric": f"ms per {L}x{L}-limb NTT product ({args.ntt_path})", "value": ms, "unit": "ms",
                           "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
                           "a_b_ret_GBps": 16.0 * L / (ms * 1e-3) / 1e9, "kernel_families": fam}), flush=True)
     ctx.close()
@@ -537,6 +550,8 @@ def main():
                     help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step; "
                          "convert: one 2^25-limb decimal conversion per step; uneven: 4096 uneven products")
     ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
+    ap.add_argument("--ntt-path", choices=["fused", "spectra"], default="fused",
+                    help="ntt workload: fused row pass, or forward / inverse spectra")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if ws > 1:
