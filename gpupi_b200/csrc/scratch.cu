@@ -24,6 +24,7 @@
 //
 // Blocks are released when the last BatchMPContext is destroyed.
 #include "common.cuh"
+#include "range_map.h"
 
 #include <map>
 #include <mutex>
@@ -42,58 +43,23 @@ struct Arena {
     cudaStream_t stream = nullptr;
     char *base = nullptr;
     size_t cap = 0;
-    std::map<size_t, size_t> free_at;               // offset -> size
-    std::multimap<size_t, size_t> free_by_size;     // size -> offset
+    RangeMap free;                                  // free ranges of the block
     std::unordered_map<void *, size_t> live;        // arena blocks: ptr -> size
     std::unordered_map<void *, size_t> spilled;     // cudaMallocAsync blocks: ptr -> size
     size_t live_bytes = 0, high = 0;
     uint64_t spills = 0;   // requests ever served outside the block
     bool grow = false;
 
-    void erase_free(size_t off, size_t size) {
-        free_at.erase(off);
-        auto r = free_by_size.equal_range(size);
-        for (auto it = r.first; it != r.second; ++it)
-            if (it->second == off) {
-                free_by_size.erase(it);
-                return;
-            }
-    }
-    void insert_free(size_t off, size_t size) {
-        auto next = free_at.lower_bound(off);
-        if (next != free_at.end() && off + size == next->first) {
-            const size_t noff = next->first, nsize = next->second;
-            erase_free(noff, nsize);
-            size += nsize;
-        }
-        auto it = free_at.lower_bound(off);
-        if (it != free_at.begin()) {
-            auto prev = std::prev(it);
-            if (prev->first + prev->second == off) {
-                const size_t poff = prev->first, psize = prev->second;
-                erase_free(poff, psize);
-                off = poff;
-                size += psize;
-            }
-        }
-        free_at[off] = size;
-        free_by_size.emplace(size, off);
-    }
     void reset_block(char *p, size_t bytes) {
         base = p;
-        cap = bytes;
-        free_at.clear();
-        free_by_size.clear();
-        if (p) insert_free(0, bytes);
+        cap = p ? bytes : 0;
+        free.reset(cap);
     }
 
     cudaError_t alloc(void **out, size_t bytes) {
         const size_t need = round_up(bytes ? bytes : 1, kAlign);
-        auto it = free_by_size.lower_bound(need);
-        if (it != free_by_size.end()) {
-            const size_t size = it->first, off = it->second;
-            erase_free(off, size);
-            if (size > need) insert_free(off + need, size - need);
+        size_t off = 0;
+        if (base && free.take(need, &off)) {
             void *p = base + off;
             live.emplace(p, need);
             live_bytes += need;
@@ -117,7 +83,7 @@ struct Arena {
     bool release(void *p) {
         auto a = live.find(p);
         if (a != live.end()) {
-            insert_free((size_t)((char *)p - base), a->second);
+            free.give((size_t)((char *)p - base), a->second);
             live_bytes -= a->second;
             live.erase(a);
         } else {
