@@ -225,8 +225,9 @@ def run_reference_arm(args, ws, rank):
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (pi has no input data)",
-        "config": {"workload": f"pi to {args.digits} digits", "sample_digits_per_step": d,
-                   "l2": "inputs larger than L2"},
+        "config": {"workload": f"pi to {args.digits} decimal digits (pi_bs_gpu {args.digits})",
+                   "digits": args.digits, "sample_digits_per_step": d,
+                   "l2": "working set larger than L2; no flush needed"},
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
                          "sample": f"pi to {d} digits per step with {what} (the reference has no CPU "
                                    f"implementation), mean of {args.steps} steps scaled linearly to "
