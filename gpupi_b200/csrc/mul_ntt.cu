@@ -613,6 +613,102 @@ __global__ void __launch_bounds__((1 << kSplitLogC) / 16, 4) k_rows_inv(NttParam
     }
 }
 
+// One merge level's four row products in one pass (the tuned form's level):
+// from the column-transformed segments of P_e, P_o, R_o, Q_o, Q_e, R_e the
+// CTA forms P' = P_e P_o, R2 = P_e R_o, Q' = Q_e Q_o, R1 = R_e Q_o (each
+// x K^-1) and runs their inverse row stages, writing them over P_o, R_o, Q_e
+// and R_e: six forward and four inverse row transforms, the kept operand
+// (P_e, then Q_o) and one product in registers, no spectrum stored.
+struct RowsLevelArgs {
+    uint32_t *Fpe, *Fpo, *Fro, *Fqo, *Fqe, *Fre;
+    int log_k;
+};
+
+template <int Q>
+__device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLevelArgs &a, uint64_t b,
+                                                uint32_t *Sm, uint2 *tw, uint32_t *held) {
+    constexpr int C = 1 << kSplitLogC;
+    constexpr int T = C / 16;
+    using First = typename ExecStage<kSplitLogC, 0, false, 0>::S;
+    using Out = typename ExecStage<kSplitLogC, 0, true, StagePlan<kSplitLogC>::n - 1>::S;
+    const uint32_t nseg = 1u << (a.log_k - kSplitLogC);
+    const uint64_t K = 1ull << a.log_k;
+    const uint64_t off = (b / nseg) * 3 * K + (uint64_t)Q * K + ((uint64_t)(b % nseg) << kSplitLogC);
+    const uint32_t t = threadIdx.x;
+    const uint32_t scale = __ldg(P.tab.inv2n + a.log_k * kPrimes + Q);
+    const uint2 *levf = level_ptr(P.tab, 0, Q);
+    const uint2 *levi = level_ptr(P.tab, 1, Q);
+    auto load = [&](const uint32_t *F, uint32_t (&x)[16]) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            First::elem(t, j, pos, c);
+            x[j] = __ldg(F + off + pos);
+        }
+    };
+    auto store = [&](uint32_t *F, const uint32_t (&x)[16]) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t pos, c;
+            Out::elem(t, j, pos, c);
+            F[off + pos] = x[j];
+        }
+    };
+    auto table = [&](const uint2 *lev) {
+        __syncthreads();   // the previous stages have left the tile and the table
+        for (uint32_t e = t; e < C - 1; e += T) tw[e] = __ldg(lev + e);
+        __syncthreads();
+    };
+    // kept operand F_keep; products F_keep F0 -> F0, F_keep F1 -> F1.  The
+    // first product waits in the thread's own slots of `held` (word j of
+    // thread t at j * T + t: conflict-free) while the second is formed.
+    auto half = [&](const uint32_t *F_keep, uint32_t *F0, uint32_t *F1) {
+        uint32_t k[16], x[16];
+        table(levf);
+        load(F_keep, k);
+        run_stages<kSplitLogC, 0, false, Q, 0>(k, Sm, t, tw);
+        __syncthreads();
+        load(F0, x);
+        run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) held[j * T + t] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
+        __syncthreads();
+        load(F1, x);
+        run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
+        table(levi);
+        run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
+        store(F1, x);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = held[j * T + t];
+        run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
+        store(F0, x);
+    };
+    half(a.Fpe, a.Fpo, a.Fro);
+    half(a.Fqo, a.Fqe, a.Fre);
+}
+
+// the padded tile, the twiddle levels, one held product
+constexpr size_t rows_level_smem_bytes() { return rows_smem_bytes<kSplitLogC>() + (size_t)(1 << kSplitLogC) * 4u; }
+
+__global__ void __launch_bounds__((1 << kSplitLogC) / 16, 3) k_rows_level(NttParams P, RowsLevelArgs a) {
+    extern __shared__ uint4 rows_smem[];
+    constexpr int C = 1 << kSplitLogC;
+    uint32_t *Sm = reinterpret_cast<uint32_t *>(rows_smem);
+    uint2 *tw = reinterpret_cast<uint2 *>(Sm + C + C / 32);
+    uint32_t *held = reinterpret_cast<uint32_t *>(tw + (C - 1));
+    uint64_t b;
+    const int q = grid_prime(b);
+    if (q == 0)
+        rows_level_body<0>(P, a, b, Sm, tw, held);
+    else if (q == 1)
+        rows_level_body<1>(P, a, b, Sm, tw, held);
+    else
+        rows_level_body<2>(P, a, b, Sm, tw, held);
+}
+
 // Coset recombination.  Row r holds z_i[j] = C_i[j] g^(ij) for cosets i < M;
 // C_i[j] = sum_b C_b[j] c_i^b, so C_b[j] = sum_i Vinv[b][i] C_i[j].  The M
 // outputs of position j overwrite the M inputs of position j.
@@ -1101,13 +1197,15 @@ static void rows_split_attr() {
         cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         cudaFuncSetAttribute(k_rows_inv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         cudaFuncSetAttribute(k_rows_inv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_rows_level, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rows_level_smem_bytes());
         done = true;
     }
 }
 
 static void spectrum_forward(const NttParams &P, Shape s, uint32_t N, const uint32_t *X, uint64_t sX, uint32_t Lx,
                              uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly, uint32_t *FY,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool rows) {
     const int log_k = s.log_k, M = s.M;
     const uint64_t K = 1ull << log_k;
     const uint64_t VR = (uint64_t)N * M;
@@ -1128,6 +1226,7 @@ static void spectrum_forward(const NttParams &P, Shape s, uint32_t N, const uint
             log_s -= passes[ps];
         }
     }
+    if (!rows) return;
     rows_split_attr();
     RowsFwdArgs r{FX, Y ? FY : nullptr, log_k};
     const unsigned blocks = (unsigned)(VR * kPrimes * (K >> kSplitLogC));
@@ -1138,11 +1237,12 @@ static void spectrum_forward(const NttParams &P, Shape s, uint32_t N, const uint
 
 static void spectrum_inverse(const NttParams &P, Shape s, uint32_t N, int terms, const uint32_t *const *X,
                              const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC, uint32_t Lc,
-                             uint32_t *flags, cudaStream_t st) {
+                             uint32_t *flags, cudaStream_t st, bool rows) {
     const int log_k = s.log_k, M = s.M;
     const uint64_t K = 1ull << log_k;
     const uint64_t VR = (uint64_t)N * M;
     rows_split_attr();
+    if (rows) {
     RowsInvArgs r{};
     for (int i = 0; i < terms; ++i) {
         r.X[i] = X[i];
@@ -1159,6 +1259,7 @@ static void spectrum_inverse(const NttParams &P, Shape s, uint32_t N, int terms,
         else
             k_rows_inv<2><<<blocks, (1 << kSplitLogC) / 16, rows_smem_bytes<kSplitLogC>(), st>>>(P, r);
         count_launch();
+    }
     }
     int passes[2];
     const int npass = column_passes(log_k, passes);
@@ -1292,16 +1393,30 @@ bool spectrum_sum_fits(const uint32_t *La, const uint32_t *Lb, int terms) {
 
 void spectrum_forward(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, const uint32_t *X,
                       uint64_t sX, uint32_t Lx, uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly,
-                      uint32_t *FY) {
+                      uint32_t *FY, bool rows) {
     const ntt::NttParams P = ntt::make_params(tables);
-    ntt::spectrum_forward(P, ntt::Shape{s.log_k, s.M}, N, X, sX, Lx, FX, Y, sY, Ly, FY, current_stream());
+    ntt::spectrum_forward(P, ntt::Shape{s.log_k, s.M}, N, X, sX, Lx, FX, Y, sY, Ly, FY, current_stream(), rows);
 }
 
 void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, int terms,
                       const uint32_t *const *X, const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC,
-                      uint32_t Lc, uint32_t *flags) {
+                      uint32_t Lc, uint32_t *flags, bool rows) {
     const ntt::NttParams P = ntt::make_params(tables);
-    ntt::spectrum_inverse(P, ntt::Shape{s.log_k, s.M}, N, terms, X, Y, Fout, C, sC, Lc, flags, current_stream());
+    ntt::spectrum_inverse(P, ntt::Shape{s.log_k, s.M}, N, terms, X, Y, Fout, C, sC, Lc, flags, current_stream(),
+                          rows);
+}
+
+void spectrum_level_rows(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, uint32_t *Fpe,
+                         uint32_t *Fpo, uint32_t *Fro, uint32_t *Fqo, uint32_t *Fqe, uint32_t *Fre) {
+    const ntt::NttParams P = ntt::make_params(tables);
+    cudaStream_t st = current_stream();
+    ntt::rows_split_attr();
+    const uint64_t VR = (uint64_t)N * s.M;
+    const unsigned blocks = (unsigned)(VR * ntt::kPrimes * ((1ull << s.log_k) >> ntt::kSplitLogC));
+    ntt::RowsLevelArgs a{Fpe, Fpo, Fro, Fqo, Fqe, Fre, s.log_k};
+    KernelTimed kt("ntt_rows_level", 40.0 * (double)(1ull << s.log_k) * (double)VR * ntt::kPrimes);
+    ntt::k_rows_level<<<blocks, (1 << ntt::kSplitLogC) / 16, ntt::rows_level_smem_bytes(), st>>>(P, a);
+    count_launch();
 }
 
 }  // namespace gpupi

@@ -257,8 +257,10 @@ static cudaError_t plain_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
 // One merge level with shared forward transforms (the tuned form of
 // pi_bs_gpu.cu:625-723): Q_o serves Q' = Q_e Q_o and R1 = R_e Q_o, P_e
 // serves P' = P_e P_o and R2 = P_e R_o, so the level's four products take
-// six forward transforms instead of eight (four inverse either way); then
-// R' = (R1 << s) +- R2 as in the plain level.  Used when all four products
+// six forward transforms instead of eight (four inverse either way): the
+// six operands' column passes, then one row kernel for the four products
+// (spectrum_level_rows), then each product's inverse column passes and
+// CRT; R' = (R1 << s) +- R2 as in the plain level.  Used when all four products
 // have the same transform shape (summing R' in the transform domain would
 // need room for R1 << s, about 6 % longer than R1, which sits just below a
 // power of two at every level and would double the transforms).  The
@@ -287,66 +289,54 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
     const BatchMPArray R_even{R.data, lr, half, R.stride * 2}, R_odd{R.data + R.stride, lr, half, R.stride * 2};
     Buf fpe, fpo, fqe, fqo, fre, fro, flags, r1b, r2b;
     TRY(flags.alloc(spectrum_flag_words(half, std::max(std::max(lr + lq, 2u * lq), std::max(lr + lp, 2u * lp)))));
-    auto product = [&](const char *label, uint32_t rows, const Buf &fx, const Buf &fy, uint32_t *C, uint32_t Lc,
-                       uint32_t la, uint32_t lb) {
+    // column passes of the six operands, two per launch: P_e and P_o share
+    // the pb rows they both have (P_e's last row follows alone when P has an
+    // odd row count; P_o's row there is left unset and its product unused)
+    TRY(stage(pr, "fwd", "P,Q,R columns", n1, half, lp, lq, true, [&]() {
+        TRY(fpe.alloc(words));
+        TRY(fpo.alloc(words));
+        TRY(fqo.alloc(words));
+        TRY(fqe.alloc(words));
+        TRY(fre.alloc(words));
+        TRY(fro.alloc(words));
+        spectrum_forward(tab, S, pb, P_even.data, P_even.stride, lp, fpe.p, P_odd.data, P_odd.stride, lp, fpo.p,
+                         false);
+        if (pb < half)
+            spectrum_forward(tab, S, 1u, P_even.data + (size_t)pb * P_even.stride, P_even.stride, lp,
+                             fpe.p + spectrum_words(S, pb), nullptr, 0, 0, nullptr, false);
+        spectrum_forward(tab, S, half, Q_odd.data, Q_odd.stride, lq, fqo.p, Q_even.data, Q_even.stride, lq, fqe.p,
+                         false);
+        spectrum_forward(tab, S, half, R_even.data, R_even.stride, lr, fre.p, R_odd.data, R_odd.stride, lr, fro.p,
+                         false);
+        // the four products' row passes in one kernel
+        spectrum_level_rows(tab, S, half, fpe.p, fpo.p, fro.p, fqo.p, fqe.p, fre.p);
+        fpe.reset();
+        fqo.reset();
+        return cudaGetLastError();
+    }));
+    auto finish = [&](const char *label, uint32_t rows, Buf &f, uint32_t *C, uint32_t Lc, uint32_t la,
+                      uint32_t lb) {
         return stage(pr, "mul", label, n1, rows, la, lb, true, [&]() {
-            const uint32_t *X[1] = {fx.p}, *Y[1] = {fy.p};
-            spectrum_inverse(tab, S, rows, 1, X, Y, fx.p, C, Lc, Lc, flags.p);
+            spectrum_inverse(tab, S, rows, 1, nullptr, nullptr, f.p, C, Lc, Lc, flags.p, false);
+            f.reset();
             return cudaGetLastError();
         });
     };
-    // P' = P_e P_o (P_e kept for R2)
-    // P_e and P_o share one launch per pass for the pb rows they both have;
-    // when P has an odd row count (pb = half - 1) P_e's last row follows alone
-    TRY(stage(pr, "fwd", "P_e,P_o", n1, half, lp, lp, true, [&]() {
-        TRY(fpe.alloc(words));
-        TRY(fpo.alloc(words));
-        spectrum_forward(tab, S, pb, P_even.data, P_even.stride, lp, fpe.p, P_odd.data, P_odd.stride, lp, fpo.p);
-        if (pb < half)
-            spectrum_forward(tab, S, 1u, P_even.data + (size_t)pb * P_even.stride, P_even.stride, lp,
-                             fpe.p + spectrum_words(S, pb), nullptr, 0, 0, nullptr);
-        return cudaGetLastError();
-    }));
     Pn = BatchMPArray{nullptr, 2u * lp, pb, 2u * lp};
     TRY(pn.alloc((size_t)pb * Pn.stride));
     Pn.data = pn.p;
-    // P_e's spectrum is needed again for R2: the product writes into P_o's
-    TRY(stage(pr, "mul", "P", n1, pb, lp, lp, true, [&]() {
-        const uint32_t *X[1] = {fpo.p}, *Y[1] = {fpe.p};
-        spectrum_inverse(tab, S, pb, 1, X, Y, fpo.p, Pn.data, Pn.stride, Pn.length, flags.p);
-        return cudaGetLastError();
-    }));
-    fpo.reset();
+    TRY(finish("P", pb, fpo, Pn.data, Pn.length, lp, lp));
     TRY(p_compact(ctx, pr, Pn, "P", n1));
-    // Q' = Q_e Q_o (Q_o kept for R1)
-    TRY(stage(pr, "fwd", "Q_o,Q_e", n1, half, lq, lq, true, [&]() {
-        TRY(fqo.alloc(words));
-        TRY(fqe.alloc(words));
-        spectrum_forward(tab, S, half, Q_odd.data, Q_odd.stride, lq, fqo.p, Q_even.data, Q_even.stride, lq, fqe.p);
-        return cudaGetLastError();
-    }));
     Qn = BatchMPArray{nullptr, 2u * lq, half, 2u * lq};
     TRY(qn.alloc((size_t)half * Qn.stride));
     Qn.data = qn.p;
-    TRY(product("Q", half, fqe, fqo, Qn.data, Qn.length, lq, lq));
-    fqe.reset();
+    TRY(finish("Q", half, fqe, Qn.data, Qn.length, lq, lq));
     TRY(p_compact(ctx, pr, Qn, "Q", n1));
-    // R1 = R_e Q_o, R2 = P_e R_o
-    TRY(stage(pr, "fwd", "R_e,R_o", n1, half, lr, lr, true, [&]() {
-        TRY(fre.alloc(words));
-        TRY(fro.alloc(words));
-        spectrum_forward(tab, S, half, R_even.data, R_even.stride, lr, fre.p, R_odd.data, R_odd.stride, lr, fro.p);
-        return cudaGetLastError();
-    }));
     const BatchMPArray R1{nullptr, lr + lq, half, lr + lq}, R2{nullptr, lr + lp, half, lr + lp};
     TRY(r1b.alloc((size_t)half * R1.stride));
     TRY(r2b.alloc((size_t)half * R2.stride));
-    TRY(product("R*Q", half, fre, fqo, r1b.p, R1.length, lr, lq));
-    TRY(product("P*R", half, fro, fpe, r2b.p, R2.length, lp, lr));
-    fre.reset();
-    fro.reset();
-    fqo.reset();
-    fpe.reset();
+    TRY(finish("R*Q", half, fre, r1b.p, R1.length, lr, lq));
+    TRY(finish("P*R", half, fro, r2b.p, R2.length, lp, lr));
     const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
     const uint32_t r1_shifted = R1.length + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
     const uint32_t rlen = std::max(r1_shifted, R2.length) + (subtract ? 0u : 1u);

@@ -32,14 +32,24 @@ bool spectrum_sum_fits(const uint32_t *La, const uint32_t *Lb, int terms);
 
 // FX (and FY when Y is not null) = forward transforms of N rows of X (Y);
 // rows at X + i * sX, Lx limbs (zero above).
+// rows = false: the column passes only (for spectrum_level_rows).
 void spectrum_forward(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, const uint32_t *X,
                       uint64_t sX, uint32_t Lx, uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly,
-                      uint32_t *FY);
+                      uint32_t *FY, bool rows = true);
 // C rows (stride sC, Lc limbs) = sum over terms (<= 2) of X_t Y_t.  Fout
 // receives the intermediate residues and may be one of the X_t / Y_t;
 // flags: spectrum_flag_words(N, Lc) words.
+// rows = false: Fout already holds the product after its inverse row pass
+// (spectrum_level_rows); X and Y are not read.
 void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, int terms,
                       const uint32_t *const *X, const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC,
-                      uint32_t Lc, uint32_t *flags);
+                      uint32_t Lc, uint32_t *flags, bool rows = true);
+
+// One merge level's row products from six column-transformed operands
+// (spectrum_forward with rows = false): P' = P_e P_o into Fpo, R2 = P_e R_o
+// into Fro, Q' = Q_e Q_o into Fqe, R1 = R_e Q_o into Fre, each after its
+// inverse row pass; N rows of shape s.
+void spectrum_level_rows(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, uint32_t *Fpe,
+                         uint32_t *Fpo, uint32_t *Fro, uint32_t *Fqo, uint32_t *Fqe, uint32_t *Fre);
 
 }  // namespace gpupi
