@@ -43,14 +43,17 @@ ROOT = Path(__file__).resolve().parent
 # pi run's launches are scaled by their algorithmic bytes.
 BBP_POSITIONS = 64
 # DRAM bytes (read + write) over algorithmic bytes of one launch, from ncu
-# captures on 2^22 x 2^22-limb products (profiles/ntt_rows_cols_4Mi.md,
-# profiles/ntt_split_rows_4Mi.md); applied to each launch of the family
+# captures (profiles/ntt_rows_cols_4Mi.md, profiles/ntt_split_rows_4Mi.md,
+# profiles/ntt_rows_level_pi1e8.md); applied to each launch of the family
 NCU_TRAFFIC_RATIO = {"ntt_rows_fused": 264.006 / 301.990,
-                     "ntt_cols_fwd_first": 229.642496 / 234.881024}
+                     "ntt_cols_fwd_first": 229.642496 / 234.881024,
+                     "ntt_rows_level": (2417.13 + 1586.67) / 4026.531840}
 NCU_TRAFFIC_SOURCE = {"ntt_rows_fused": "ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product, "
                                         "scaled to each launch by its algorithmic bytes",
                       "ntt_cols_fwd_first": "ncu capture of k_cols_r<6, first, fwd, pair> on a 2^22 x 2^22-limb "
-                                            "product, scaled to each launch by its algorithmic bytes"}
+                                            "product, scaled to each launch by its algorithmic bytes",
+                      "ntt_rows_level": "ncu capture of k_rows_level in pi to 1e8 digits (2^25 points x 3 primes "
+                                        "per launch), scaled to each launch by its algorithmic bytes"}
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ms to 1e9 digits of pi (bit-exact), tuned vs plain form on B200; NTT HBM GB/s"
