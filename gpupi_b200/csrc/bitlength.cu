@@ -1,8 +1,9 @@
 // Largest used bit / limb length over a batch (gpupi batch_bitlength.cu:33-245).
 //
-// Few rows: 4096-limb chunks scanned from the top by all CTAs, skipping
-// chunks that cannot beat the best length found so far.  Many rows: one
-// thread per row, bounded by the best length seen so far.  Per-CTA maxima meet in one device word; the
+// Long rows (unless there are very many): 4096-limb chunks scanned from the
+// top by all CTAs, skipping chunks that cannot beat the best length found so
+// far.  Short rows, or very many rows: one thread per row, bounded by the
+// best length seen so far.  Per-CTA maxima meet in one device word; the
 // last CTA to finish (ticket counter) moves the result straight into pinned,
 // mapped host memory and re-zeroes the word and the counter, so a call is one
 // launch plus one stream synchronisation — no memset, no device-to-host copy.
@@ -171,7 +172,12 @@ static uint32_t length_max(const uint32_t *A, uint32_t *workspace, uint32_t N, u
     if (!s) return 0u;
     cudaStream_t st = current_stream();
     *s->host = 0xffffffffu;
-    if (N >= 4096u)
+    // one thread per row only for short rows or very many rows: a thread
+    // reads its row from the top one limb at a time, which for rows of
+    // thousands of limbs that are shorter than the batch's length is a long
+    // serial scan (up to 7 ms for 4096 rows of 60K limbs); the chunked
+    // kernel reads such rows in coalesced 4096-limb chunks
+    if (L <= 64u || N >= 65536u)
         length_max_rows_kernel<BITS><<<grid_for(N, 256, kNumSMs * 8), 256, 0, st>>>(A, N, L, stride, s->dev,
                                                                                   s->dev + 1, s->host_dev);
     else {

@@ -144,7 +144,10 @@ def test_exactdiv(ctx, divisor):
 
 def test_bitlength(ctx):
     rng = np.random.default_rng(3)
-    for (N, L, stride) in [(1, 1, 1), (100, 17, 20), (5, 9000, 9000), (40000, 3, 3)]:
+    # both kernels: chunked (long rows, or few rows) and one thread per row
+    # (short rows, or 65536 rows and more)
+    for (N, L, stride) in [(1, 1, 1), (100, 17, 20), (5, 9000, 9000), (40000, 3, 3), (5000, 100, 101),
+                           (4096, 3000, 3000), (70000, 70, 70), (8192, 64, 64)]:
         A = rand_buf(rng, N, stride, L)
         for r in range(N):
             cut = int(rng.integers(0, L + 1))
@@ -155,6 +158,14 @@ def test_bitlength(ctx):
     Z = np.zeros(64, dtype=np.uint32)
     dZ = to_dev(Z)
     assert ctx.limblength_max(4, dZ.ptr, 16, 16) == 0
+    # many long rows, all but one far shorter than the batch length
+    N, L = 4096, 20000
+    A = np.zeros(N * L, dtype=np.uint32)
+    A[np.arange(N) * L + 7] = 1
+    A[1234 * L + 19000] = 5
+    dA = to_dev(A)
+    assert ctx.limblength_max(N, dA.ptr, L, L) == 19001
+    assert ctx.bitlength_max(N, dA.ptr, L, L) == 19000 * 32 + 3
 
 
 def test_invalid_metadata(ctx):
