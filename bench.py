@@ -378,6 +378,9 @@ def run_ours(args, ws, rank, local):
                            "otherwise the reference's op sequence, one op per launch, compact after every op)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "working set (tens of GB) larger than L2; no flush needed"},
+        "whole_job": {"digits_per_s": ws * digits / (ms * 1e-3), "pi_runs_per_s": ws / (ms * 1e-3),
+                      "note": "each GPU computes its own 1e9-digit pi per step (replicas); value is the "
+                              "max-over-ranks time of one step, so ideal weak scaling keeps it constant"},
         "forms": {"tuned_ms": ms, "plain_ms": ms_plain, "plain_over_tuned": ms_plain / ms,
                   "plain_ret_len": rp.ret_len},
         "pipeline_elapsed_ms": statistics.mean(inner),
