@@ -138,7 +138,8 @@ def _max_over_ranks(x: float, ws: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -565,8 +566,12 @@ def main():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # NCCL between the GPUs; gloo when there is no GPU (the reference arm
+        # and the multi-rank plumbing run on host cores)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     try:
         if args.impl == "reference":
             run_reference_arm(args, ws, rank)
