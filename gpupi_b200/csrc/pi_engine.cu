@@ -15,6 +15,7 @@
 #include "convert_decimal.h"
 #include "pi_engine.h"
 #include "spectrum.h"
+#include "checkpoint_file.h"
 
 #include <math.h>
 #include <stdio.h>
@@ -711,50 +712,21 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
 // pi_fractional (pi_bs_gpu.cu:1524-1685)
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
-// Checkpoint of the splitting tree's result (Q and R of 17N terms, batch 1):
-// a header {"GPUPICK1", version 1, N, Q limbs, R limbs, 64-bit checksum of
-// the limbs} followed by Q's and R's limbs, little-endian.  Written to
-// <path>.tmp and renamed, so a file that exists is complete; a load checks
-// the header, N and the checksum and otherwise leaves the tree to run.
+// Checkpoint of the splitting tree's result (Q and R of 17N terms, batch 1);
+// the file format is checkpoint_file.h's.
 // ---------------------------------------------------------------------------
-struct CkptHeader {
-    char magic[8];
-    uint32_t version, N, lq, lr;
-    uint64_t sum;
-};
-
-static uint64_t limb_checksum(const uint32_t *a, size_t n, uint64_t h) {
-    for (size_t i = 0; i < n; ++i) {
-        h ^= a[i];
-        h *= 0x100000001b3ull;   // FNV-1a prime, one 32-bit word per step
-        h ^= h >> 29;
-    }
-    return h;
-}
-
 static bool ckpt_load(const char *path, uint32_t N, Buf &qb, BatchMPArray &Q, Buf &rb, BatchMPArray &R) {
-    FILE *f = fopen(path, "rb");
-    if (!f) return false;
-    CkptHeader h{};
-    bool ok = fread(&h, sizeof h, 1, f) == 1 && memcmp(h.magic, "GPUPICK1", 8) == 0 && h.version == 1u &&
-              h.N == N && h.lq > 0u && h.lr > 0u;
     std::vector<uint32_t> q, r;
-    if (ok) {
-        q.resize(h.lq);
-        r.resize(h.lr);
-        ok = fread(q.data(), 4, h.lq, f) == h.lq && fread(r.data(), 4, h.lr, f) == h.lr && fgetc(f) == EOF;
-    }
-    fclose(f);
-    if (!ok || limb_checksum(r.data(), h.lr, limb_checksum(q.data(), h.lq, 0xcbf29ce484222325ull)) != h.sum)
-        return false;
+    if (!ckpt_read(path, N, q, r)) return false;
+    const uint32_t lq = (uint32_t)q.size(), lr = (uint32_t)r.size();
     cudaStream_t st = current_stream();
-    if (qb.alloc(h.lq) != cudaSuccess || rb.alloc(h.lr) != cudaSuccess) return false;
-    Q = BatchMPArray{qb.p, h.lq, 1, h.lq};
-    R = BatchMPArray{rb.p, h.lr, 1, h.lr};
-    ok = cudaMemcpyAsync(Q.data, q.data(), (size_t)h.lq * 4, cudaMemcpyHostToDevice, st) == cudaSuccess &&
-         cudaMemcpyAsync(R.data, r.data(), (size_t)h.lr * 4, cudaMemcpyHostToDevice, st) == cudaSuccess &&
-         cudaStreamSynchronize(st) == cudaSuccess;
-    note_h2d(((size_t)h.lq + h.lr) * 4);
+    if (qb.alloc(lq) != cudaSuccess || rb.alloc(lr) != cudaSuccess) return false;
+    Q = BatchMPArray{qb.p, lq, 1, lq};
+    R = BatchMPArray{rb.p, lr, 1, lr};
+    const bool ok = cudaMemcpyAsync(Q.data, q.data(), (size_t)lq * 4, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+                    cudaMemcpyAsync(R.data, r.data(), (size_t)lr * 4, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+                    cudaStreamSynchronize(st) == cudaSuccess;
+    note_h2d(((size_t)lq + lr) * 4);
     return ok;
 }
 
@@ -765,21 +737,7 @@ static cudaError_t ckpt_save(const char *path, uint32_t N, const BatchMPArray &Q
     TRY(cudaMemcpyAsync(r.data(), R.data, (size_t)R.length * 4, cudaMemcpyDeviceToHost, st));
     TRY(cudaStreamSynchronize(st));
     note_d2h(((size_t)Q.length + R.length) * 4);
-    CkptHeader h{};
-    memcpy(h.magic, "GPUPICK1", 8);
-    h.version = 1u;
-    h.N = N;
-    h.lq = Q.length;
-    h.lr = R.length;
-    h.sum = limb_checksum(r.data(), r.size(), limb_checksum(q.data(), q.size(), 0xcbf29ce484222325ull));
-    const std::string tmp = std::string(path) + ".tmp";
-    FILE *f = fopen(tmp.c_str(), "wb");
-    if (!f) return cudaErrorInvalidValue;
-    bool ok = fwrite(&h, sizeof h, 1, f) == 1 && fwrite(q.data(), 4, q.size(), f) == q.size() &&
-              fwrite(r.data(), 4, r.size(), f) == r.size();
-    ok = (fclose(f) == 0) && ok && rename(tmp.c_str(), path) == 0;
-    if (!ok) remove(tmp.c_str());
-    return ok ? cudaSuccess : cudaErrorInvalidValue;
+    return ckpt_write(path, N, q, r) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, Buf &retbuf, BatchMPArray &RET,
