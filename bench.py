@@ -18,9 +18,17 @@ Our arm (``--impl ours``):
              algorithmic bytes / its event-timed duration, against the
              measured HBM copy bandwidth;
   cpu_baseline  the CPU restatement (oracle) on a bounded sample, rank 0.
-The reference arm (``--impl reference``) times the CPU restatement of the
-same pipeline (the reference ships no CPU implementation) on a bounded
-sample per step, extrapolated linearly to the metric's digit count.
+  reference_gpu_build  gpupi's own CUDA build (oracle/_ref/pi_bs_gpu_ref,
+             compiled from the reference's sources) and this library's CLI
+             run alternately as cold processes, `--benchmark`, same digits:
+             each program's own elapsed_ms and RET hash (rank 0, after the
+             timed regions).
+The reference arm (``--impl reference``) runs gpupi's own CUDA build,
+``pi_bs_gpu_ref <digits> --benchmark``, one cold process per step on rank 0's
+GPU, and reports its own elapsed_ms (CUDA events around the same pipeline,
+digits left on the device, like ``value``).  Where that build is absent it
+times the host C++ restatement instead (the reference has no CPU
+implementation) and says so.
 """
 from __future__ import annotations
 
@@ -198,11 +206,80 @@ def cpu_baseline_sample(digits: int) -> dict:
             "sample_ms": ms}
 
 
-def run_reference_arm(args, ws, rank):
-    """The reference has no CPU implementation of the pipeline; its arm times
-    the host C++ restatement (GMP, all host threads), the same recurrence and
-    the same RET, on a bounded sample per step scaled to the metric."""
+REF_CLI = ROOT / "oracle" / "_ref" / "pi_bs_gpu_ref"
+OUR_CLI = ROOT / "gpupi_b200" / "pi_bs_gpu"
+REF_FIXTURES = ROOT / "tests" / "golden" / "ref_fixtures.json"
+
+
+def _cli_benchmark(exe: Path, digits: int, device: int) -> dict:
+    """One cold `<exe> <digits> --benchmark` process: its own elapsed_ms, RET
+    length and RET hash (pi_bs_gpu.cu:2216-2224 format), and the wall time."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=str(device))
+    t0 = time.perf_counter()
+    r = subprocess.run([str(exe), str(digits), "--benchmark"], capture_output=True, text=True, env=env,
+                       timeout=900)
+    wall = (time.perf_counter() - t0) * 1e3
+    if r.returncode != 0:
+        raise RuntimeError(f"{exe.name} {digits} --benchmark exited {r.returncode}: {r.stderr[-500:]}")
+    lines = r.stdout.splitlines()
+    f = dict(kv.split("=", 1) for kv in lines[0].split() if "=" in kv)
+    ret_line = next(l for l in lines if l.startswith("RET = "))
+    return {"elapsed_ms": float(f["elapsed_ms"]), "ret_len": int(f["RET_len"]),
+            "ret_hash": int(ret_line.rsplit("=", 1)[1]), "wall_ms": wall}
+
+
+def _ref_fixture(digits: int) -> dict | None:
+    """The reference build's recorded result for this digit count, if any."""
+    if not REF_FIXTURES.exists():
+        return None
+    for e in json.loads(REF_FIXTURES.read_text()).get("pi", []):
+        if e["digits"] == digits:
+            return e
+    return None
+
+
+def _gpu_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def run_reference_arm(args, ws, rank, local):
+    """gpupi's own CUDA build, one cold `pi_bs_gpu_ref <digits> --benchmark`
+    process per step on this rank's GPU (rank 0 only), timed by its own
+    device events; its RET is checked against the recorded fixture.  Without
+    that build (or a GPU) the arm times the host C++ restatement instead."""
     if rank != 0:
+        return
+    if REF_CLI.exists() and _gpu_available():
+        for _ in range(args.warmup):
+            _cli_benchmark(REF_CLI, args.digits, local)
+        runs = [_cli_benchmark(REF_CLI, args.digits, local) for _ in range(args.steps)]
+        ms = statistics.mean(r["elapsed_ms"] for r in runs)
+        fx = _ref_fixture(args.digits)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (pi has no input data)",
+            "config": {"workload": f"pi to {args.digits} decimal digits (pi_bs_gpu {args.digits})",
+                       "digits": args.digits, "program": "gpupi's pi_bs_gpu built unmodified from its sources "
+                                                          "for sm_100a (oracle/build_ref.py)",
+                       "l2": "working set larger than L2; no flush needed"},
+            "step_ms": [round(r["elapsed_ms"], 3) for r in runs],
+            "process_wall_ms": [round(r["wall_ms"], 1) for r in runs],
+            "ret_len": runs[-1]["ret_len"], "ret_hash": runs[-1]["ret_hash"],
+            "ret_matches_fixture": (None if fx is None else
+                                    all(r["ret_hash"] == fx["ret_hash"] and r["ret_len"] == fx["ret_len"]
+                                        for r in runs)),
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference",
+                             "sample": f"gpupi's own CUDA build (one host thread driving the GPU), "
+                                       f"pi_bs_gpu_ref {args.digits} --benchmark, one cold process per step, "
+                                       f"mean of its own elapsed_ms over {args.steps} steps"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     d = REF_SAMPLE_DIGITS
     use_cpp = _pi_cpu(1000) is not None
@@ -233,9 +310,10 @@ def run_reference_arm(args, ws, rank):
                    "digits": args.digits, "sample_digits_per_step": d,
                    "l2": "working set larger than L2; no flush needed"},
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
-                         "sample": f"pi to {d} digits per step with {what} (the reference has no CPU "
-                                   f"implementation), mean of {args.steps} steps scaled linearly to "
-                                   f"{args.digits} (a lower bound)"},
+                         "sample": f"pi to {d} digits per step with {what} (gpupi's own build "
+                                   f"oracle/_ref/pi_bs_gpu_ref is not present or there is no GPU; the "
+                                   f"reference has no CPU implementation), mean of {args.steps} steps scaled "
+                                   f"linearly to {args.digits} (a lower bound)"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -333,6 +411,12 @@ def run_ours(args, ws, rank, local):
         raise SystemExit(f"bench: digits do not start like pi: {head}")
     from pi_ref import mod_hash
     ret_hash = mod_hash(r.ret)
+    # RET must be the reference build's, recorded on a B200 by
+    # oracle/make_ref_fixtures.py (pi_bs_gpu.cu:2216-2224 hash)
+    fx = _ref_fixture(digits)
+    if fx is not None and (fx["ret_hash"] != ret_hash or fx["ret_len"] != r.ret_len):
+        raise SystemExit(f"bench: RET (len {r.ret_len}, hash {ret_hash}) differs from the reference build's "
+                         f"(len {fx['ret_len']}, hash {fx['ret_hash']})")
     e2e = _max_over_ranks(statistics.mean(e2e_times), ws)
 
     # independent check of RET: BBP hex digits at 64 seeded positions
@@ -370,6 +454,23 @@ def run_ours(args, ws, rank, local):
     if rank != 0:
         return
     cpu = cpu_baseline_sample(CPU_SAMPLE_DIGITS) if (ws == 1 and not args.no_cpu) else None
+    # gpupi's own CUDA build beside this library's CLI: cold processes,
+    # alternating, same digits, each program's own elapsed_ms
+    refcli = None
+    if ws == 1 and args.ref_cli_runs > 0 and REF_CLI.exists() and OUR_CLI.exists():
+        theirs, ours = [], []
+        for _ in range(args.ref_cli_runs):
+            theirs.append(_cli_benchmark(REF_CLI, digits, local))
+            ours.append(_cli_benchmark(OUR_CLI, digits, local))
+        tm = statistics.median(x["elapsed_ms"] for x in theirs)
+        om = statistics.median(x["elapsed_ms"] for x in ours)
+        refcli = {"reference_elapsed_ms": [round(x["elapsed_ms"], 3) for x in theirs],
+                  "ours_elapsed_ms": [round(x["elapsed_ms"], 3) for x in ours],
+                  "reference_median_ms": tm, "ours_median_ms": om, "reference_over_ours": tm / om,
+                  "ret_hash_equal": all(a["ret_hash"] == b["ret_hash"] == ret_hash and a["ret_len"] == b["ret_len"]
+                                        for a, b in zip(theirs, ours)),
+                  "how": f"pi_bs_gpu_ref {digits} --benchmark (gpupi built from its sources, oracle/build_ref.py) "
+                         f"and gpupi_b200/pi_bs_gpu {digits} --benchmark, alternating cold processes"}
     line = {
         "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
@@ -401,6 +502,9 @@ def run_ours(args, ws, rank, local):
         "clocks": clk,
         "cpu_baseline": cpu,
         "bbp_check": bbp,
+        "ref_fixture": (None if fx is None else {"ret_hash": fx["ret_hash"], "ret_len": fx["ret_len"],
+                                                   "match": True, "source": "tests/golden/ref_fixtures.json"}),
+        "reference_gpu_build": refcli,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
@@ -560,8 +664,15 @@ def main():
     ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
     ap.add_argument("--ntt-path", choices=["fused", "spectra"], default="fused",
                     help="ntt workload: fused row pass, or forward / inverse spectra")
+    ap.add_argument("--ref-cli-runs", type=int, default=3,
+                    help="pi workload: cold runs each of gpupi's own build and this library's CLI (0: skip)")
     args = ap.parse_args()
     ws, rank, local = _dist()
+    if args.impl == "reference":
+        # rank 0 alone runs the reference; the other ranks exit without work
+        # (no process group: nothing is exchanged)
+        run_reference_arm(args, ws, rank, local)
+        return
     if ws > 1:
         import datetime
         import torch
@@ -571,11 +682,10 @@ def main():
         backend = "nccl" if torch.cuda.is_available() else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    ok = False
     try:
-        if args.impl == "reference":
-            run_reference_arm(args, ws, rank)
-        elif args.workload == "ntt":
+        if args.workload == "ntt":
             run_ntt(args, ws, rank, local)
         elif args.workload == "convert":
             run_convert(args, ws, rank, local)
@@ -583,10 +693,14 @@ def main():
             run_uneven(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
+        ok = True
     finally:
         if ws > 1:
             import torch.distributed as dist
-            dist.barrier()
+            # the closing barrier only on success: a rank that failed must
+            # not wait in it while its peers sit in a different collective
+            if ok:
+                dist.barrier()
             dist.destroy_process_group()
 
 

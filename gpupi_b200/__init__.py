@@ -358,7 +358,8 @@ def pi_compute(digits: int, ctx: Context | None = None, copy_digits: int | None 
     give the same RET and digits.
     ``checkpoint``: a file for the splitting tree's result, loaded when valid
     for this digit count (the tree is skipped) and written otherwise;
-    ``checkpoint_state`` on the result is 1 (loaded) or 2 (written)."""
+    ``checkpoint_state`` on the result is 1 (loaded), 2 (written) or 3 (the
+    file could not be written; the result is still complete)."""
     _torch()
     l = lib()
     if copy_digits is None:

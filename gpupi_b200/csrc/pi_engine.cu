@@ -715,10 +715,17 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
 // Checkpoint of the splitting tree's result (Q and R of 17N terms, batch 1);
 // the file format is checkpoint_file.h's.
 // ---------------------------------------------------------------------------
+// Lengths outside what a tree of size N can produce are rejected: Q and R
+// hold at most 8 limbs per term (the 1e9-digit tree's hold about 3.5), and R
+// must reach past the limbs that pi_fractional shifts away (15 * 17N - 8
+// bits).
 static bool ckpt_load(const char *path, uint32_t N, Buf &qb, BatchMPArray &Q, Buf &rb, BatchMPArray &R) {
     std::vector<uint32_t> q, r;
-    if (!ckpt_read(path, N, q, r)) return false;
+    const uint64_t max_limbs = 8ull * 17ull * N + 64ull;
+    if (!ckpt_read(path, N, q, r, max_limbs)) return false;
     const uint32_t lq = (uint32_t)q.size(), lr = (uint32_t)r.size();
+    const uint64_t rlimbs = (15ull * N * 17ull - 8ull) / 32ull;
+    if ((uint64_t)lr <= rlimbs + 1ull) return false;
     cudaStream_t st = current_stream();
     if (qb.alloc(lq) != cudaSuccess || rb.alloc(lr) != cudaSuccess) return false;
     Q = BatchMPArray{qb.p, lq, 1, lq};
@@ -753,8 +760,10 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     } else {
         TRY(binary_split(ctx, pr, N, qbs, Qbs, rbs, Rbs, tuned));
         if (ckpt) {
-            TRY(ckpt_save(ckpt, N, Qbs, Rbs));
-            *ckpt_state = 2;
+            // a file that cannot be written (unwritable directory, full
+            // disk) does not fail the computation: state 3 reports it
+            *ckpt_state = ckpt_save(ckpt, N, Qbs, Rbs) == cudaSuccess ? 2 : 3;
+            cudaGetLastError();
         }
     }
     const long rts = 15l * N * 17 - 8;

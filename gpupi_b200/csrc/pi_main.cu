@@ -160,7 +160,8 @@ int main(int argc, char **argv) {
         return 1;
     }
     if (ckpt_path)
-        fprintf(stderr, "checkpoint=%s %s\n", ckpt_path, out.checkpoint == 1 ? "loaded" : "written");
+        fprintf(stderr, "checkpoint=%s %s\n", ckpt_path,
+                out.checkpoint == 1 ? "loaded" : out.checkpoint == 2 ? "written" : "not-written");
     if (out_file) {
         if (!sink.started) fputc('3', out_file);
         fputc('\n', out_file);

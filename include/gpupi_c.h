@@ -130,8 +130,10 @@ int gpupi_mp_mul_spectra(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, uint32_t
  * (Q and R, about 1 GB at 1e9 digits): when the file holds a valid result for
  * this digit count's tree (header, tree size and checksum match) it is loaded
  * and the tree is skipped, else the tree runs and the file is written
- * (through a temporary name, renamed when complete).  info[7] = 1 loaded,
- * 2 written.  No counterpart in the reference. */
+ * (through a temporary name, synced to the disk and renamed when complete).
+ * info[7] = 1 loaded, 2 written, 3 not written (the file could not be
+ * written; the computation still completes and returns 0).  No counterpart
+ * in the reference. */
 int gpupi_pi_compute_checkpointed(gpupi_ctx *ctx, uint32_t digits, uint32_t flags, const char *checkpoint,
                                   uint32_t *h_ret, size_t ret_cap, char *h_digits, size_t digits_cap,
                                   uint32_t *info);

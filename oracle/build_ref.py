@@ -1,7 +1,8 @@
 """Build the reference (gpupi) from its own sources into oracle/_ref/.
 
 Test infrastructure only.  Compiles the unmodified reference sources where
-they lie (``/root/reference``) with nvcc for sm_100a, adding two shim headers
+they lie (``--reference DIR``, else ``$GPUPI_REFERENCE_DIR``, else
+``../reference`` beside this repository) with nvcc for sm_100a, adding two shim headers
 written for this project (oracle/shim: a <cuda/warp> stand-in, since CUDA 12.9
 lacks that CUDA 13 header, and GMP's public prototypes, since the image has
 libgmp.so.10 but no gmp.h).  GMP is linked by path.  Outputs:
@@ -10,20 +11,25 @@ libgmp.so.10 but no gmp.h).  GMP is linked by path.  Outputs:
   oracle/_ref/<name>_ref             reference tests linked with the reference library
   oracle/_ref/<name>_on_gpupi_b200   the same tests linked with libgpupi_b200.so
                                      through include/ (drop-in check)
+  oracle/_ref/ref_configs_ref        oracle/ref_configs.cu (benchmark configurations
+                                     through the public API) linked with the
+                                     reference's objects (fixture generator)
+  oracle/_ref/ref_configs_on_gpupi_b200  the same program linked with libgpupi_b200.so
 
-    python oracle/build_ref.py [--tests]
+    python oracle/build_ref.py [--tests] [--reference DIR]
 """
 from __future__ import annotations
 
 import argparse
 import concurrent.futures as cf
+import os
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-REF = Path("/root/reference")
+REF = Path(os.environ.get("GPUPI_REFERENCE_DIR", str(ROOT.parent / "reference")))
 OUT = HERE / "_ref"
 SHIM = HERE / "shim"
 NVCC = "/usr/local/cuda/bin/nvcc"
@@ -73,6 +79,25 @@ def build_pi() -> Path:
     return exe
 
 
+def build_configs() -> None:
+    """oracle/ref_configs.cu linked both ways (reference objects; this library)."""
+    objdir = OUT / "obj"
+    objdir.mkdir(parents=True, exist_ok=True)
+    src = HERE / "ref_configs.cu"
+    deps = [s for s in LIB_SRCS]
+    with cf.ThreadPoolExecutor() as ex:
+        list(ex.map(lambda s: nvcc_obj(REF / s, objdir / (s + ".o"), [SHIM, REF]), deps))
+    robj = objdir / "ref_configs.o"
+    nvcc_obj(src, robj, [SHIM, REF])
+    subprocess.run([NVCC, *ARCH, "-o", str(OUT / "ref_configs_ref"), str(robj),
+                    *[str(objdir / (d + ".o")) for d in deps], GMP], check=True)
+    mine = ROOT / "gpupi_b200"
+    mobj = objdir / "ref_configs.mine.o"
+    nvcc_obj(src, mobj, [ROOT / "include"])
+    subprocess.run([NVCC, *ARCH, "-o", str(OUT / "ref_configs_on_gpupi_b200"), str(mobj), f"-L{mine}",
+                    "-lgpupi_b200", "-Xlinker", f"-rpath={mine}"], check=True)
+
+
 def build_tests() -> None:
     objdir = OUT / "obj"
     objdir.mkdir(parents=True, exist_ok=True)
@@ -106,11 +131,17 @@ def build_tests() -> None:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--tests", action="store_true", help="also build the reference tests both ways")
+    ap.add_argument("--reference", help="reference source directory")
     a = ap.parse_args()
+    global REF
+    if a.reference:
+        REF = Path(a.reference)
     if not REF.exists():
         print("reference sources not present; nothing to build", file=sys.stderr)
         return 0
     print("built", build_pi())
+    build_configs()
+    print("built ref_configs")
     if a.tests:
         build_tests()
     return 0

@@ -3,6 +3,7 @@
 // scratch directory as argv[1]; exits non-zero on the first failure.
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include <random>
 #include <string>
@@ -60,8 +61,30 @@ int main(int argc, char **argv) {
     longer.push_back(0);
     spit(path, longer);
     CHECK(!gpupi::ckpt_read(path.c_str(), 8, q2, r2));
+    // damaged length fields (header offsets 16: Q limbs, 20: R limbs): a
+    // huge length is rejected by the file-size check before any allocation;
+    // moving one word from R to Q keeps the size but not the checksum
+    auto set_u32 = [](std::vector<unsigned char> &b, size_t off, uint32_t v) { memcpy(b.data() + off, &v, 4); };
+    for (uint32_t lq : {0xFFFFFFF0u, 0x40000000u, 0u}) {
+        std::vector<unsigned char> bad = good;
+        set_u32(bad, 16, lq);
+        spit(path, bad);
+        CHECK(!gpupi::ckpt_read(path.c_str(), 8, q2, r2));
+    }
+    {
+        std::vector<unsigned char> bad = good;
+        set_u32(bad, 16, (uint32_t)q.size() + 1u);
+        set_u32(bad, 20, (uint32_t)r.size() - 1u);
+        spit(path, bad);
+        CHECK(!gpupi::ckpt_read(path.c_str(), 8, q2, r2));
+    }
     spit(path, good);
-    CHECK(gpupi::ckpt_read(path.c_str(), 8, q2, r2) && q2 == q && r2 == r);
+    CHECK(!gpupi::ckpt_read(path.c_str(), 8, q2, r2, 1233));        // R above the caller's bound
+    CHECK(gpupi::ckpt_read(path.c_str(), 8, q2, r2, 1234) && q2 == q && r2 == r);
+    // an unwritable location: the write fails cleanly and leaves nothing
+    const std::string nodir = dir + "/missing/tree.ckpt";
+    CHECK(!gpupi::ckpt_write(nodir.c_str(), 8, q, r));
+    CHECK(slurp(nodir + ".tmp").empty());
     printf("checkpoint ok\n");
     return 0;
 }

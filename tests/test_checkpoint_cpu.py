@@ -1,6 +1,8 @@
 """The tree checkpoint's file format (gpupi_b200/csrc/checkpoint_file.h),
 built with g++: round trip, atomic rename, and rejection of another tree
-size, flipped bits, truncation and trailing bytes (no GPU)."""
+size, flipped bits, truncation, trailing bytes, damaged length fields and
+lengths above the caller's bound; a write to an unwritable location fails
+cleanly (no GPU)."""
 import shutil
 import subprocess
 from pathlib import Path

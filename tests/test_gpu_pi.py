@@ -183,6 +183,11 @@ def test_checkpoint_of_the_tree(ctx, tmp_path):
     assert g.pi_compute(d, ctx, checkpoint=ck).checkpoint_state == 2
     small = g.pi_compute(20_000, ctx, checkpoint=ck)   # another tree size
     assert small.checkpoint_state == 2 and small.dec == g.pi_compute(20_000, ctx).dec
+    # a checkpoint that cannot be written does not fail the computation
+    nowhere = tmp_path / "missing-dir" / "tree.ckpt"
+    e = g.pi_compute(d, ctx, checkpoint=nowhere)
+    assert e.checkpoint_state == 3 and not nowhere.exists()
+    assert np.array_equal(e.ret, want.ret) and e.dec == want.dec
 
 
 def test_cli_checkpoint(tmp_path):
