@@ -53,6 +53,8 @@ _SIGS = [
     ("gpupi_mp_limblength_max", ctypes.c_int, [_p, _u32, _p, _u32, _u32, ctypes.POINTER(_u32)]),
     ("gpupi_mul_naive", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_mul_ntt", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
+    ("gpupi_mul_tc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
+    ("gpupi_tc_error", ctypes.c_int, []),
     ("gpupi_decimal_naive", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32]),
     ("gpupi_convert_decimal", ctypes.c_int, [_p, _p, _u32, _u32, _u32, _u32, _p]),
     ("gpupi_pi_compute", ctypes.c_int,
@@ -250,6 +252,17 @@ class Context:
 def mul_naive(N, A, La, sA, B, Lb, sB, C, sC):
     _torch()
     _check(lib().gpupi_mul_naive(N, A, La, sA, B, Lb, sB, C, sC), "batch_mul_naive")
+
+
+def mul_tc(N, A, La, sA, B, Lb, sB, C, sC):
+    """Schoolbook product on the tensor cores (int8 split-integer MMAs)."""
+    _torch()
+    _check(lib().gpupi_mul_tc(N, A, La, sA, B, Lb, sB, C, sC), "gpupi_mul_tc")
+
+
+def tc_error() -> int:
+    """Device error word of the tensor-core kernels (read and cleared)."""
+    return int(lib().gpupi_tc_error())
 
 
 def decimal_naive(N, A, L_limb, sA, out, L_dec, s_out):

@@ -20,6 +20,10 @@ struct gpupi_ctx {
 
 namespace gpupi {
 cudaError_t bbp_fractions(const uint64_t *positions, uint32_t count, uint64_t *fractions);
+cudaError_t tc_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La, uint32_t Lb,
+                   uint64_t sA, uint64_t sB, uint64_t sC);
+bool tc_fits(uint32_t La, uint32_t Lb);
+uint32_t tc_error();
 cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const uint64_t *offA, const uint32_t *La,
                        const uint32_t *B, const uint64_t *offB, const uint32_t *Lb, uint32_t *C,
                        const uint64_t *offC);
@@ -162,6 +166,15 @@ int gpupi_mul_naive(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, con
                     (int)sB, (int)sC);
     return (int)cudaGetLastError();
 }
+
+int gpupi_mul_tc(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const uint32_t *B, uint32_t Lb,
+                 uint32_t sB, uint32_t *C, uint32_t sC) {
+    if (!gpupi::tc_fits(La, Lb) || (sA && sA < La) || (sB && sB < Lb) || (N > 1u && sC < La + Lb))
+        return (int)cudaErrorInvalidValue;
+    return (int)gpupi::tc_mul(A, B, C, N, La, Lb, sA, sB, sC);
+}
+
+int gpupi_tc_error(void) { return (int)gpupi::tc_error(); }
 
 int gpupi_mp_mul_ragged(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, const uint64_t *offA, const uint32_t *La,
                         const uint32_t *B, const uint64_t *offB, const uint32_t *Lb, uint32_t *C,

@@ -80,6 +80,18 @@ int gpupi_mul_naive(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stri
 int gpupi_mul_ntt(gpupi_ctx *ctx, uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A,
                   const uint32_t *d_B, uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t stride_C);
 
+/* batch_mul_naive's operation (batch_mul_naive.h:16-25) on the tensor cores:
+ * C = A * B for N pairs by split-integer int8 MMAs (tcgen05, INT32
+ * accumulators; each 32-bit limb as four byte digits, exact).  Bit-identical
+ * to gpupi_mul_naive.  min(L_a, L_b) <= 2048 and L_a + L_b <= 8192, both
+ * nonzero; otherwise returns 1 (cudaErrorInvalidValue). */
+int gpupi_mul_tc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_A, const uint32_t *d_B,
+                 uint32_t L_b, uint32_t stride_B, uint32_t *d_C, uint32_t stride_C);
+/* Reads and clears the tensor-core kernels' device error word: 1 when a
+ * bounded wait for MMA completion ran out (the products are then
+ * incomplete), 0 otherwise.  Synchronises with the device. */
+int gpupi_tc_error(void);
+
 /* Ragged batch (no counterpart in the reference, whose batches share one
  * L_a / L_b): product i = A[offA[i] .. + L_a[i]) * B[offB[i] .. + L_b[i]) into
  * C[offC[i] .. + L_a[i] + L_b[i]).  d_A, d_B, d_C are device pointers; the
