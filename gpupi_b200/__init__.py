@@ -55,6 +55,13 @@ _SIGS = [
     ("gpupi_mul_ntt", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_mul_tc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_tc_error", ctypes.c_int, []),
+    ("gpupi_tune_load", ctypes.c_int, [ctypes.c_char_p]),
+    ("gpupi_tune_load_text", ctypes.c_int, [ctypes.c_char_p]),
+    ("gpupi_tune_reset", ctypes.c_int, []),
+    ("gpupi_tune_describe", ctypes.c_size_t, [_p, ctypes.c_size_t]),
+    ("gpupi_mul_kind", ctypes.c_int, [_u32, _u32, ctypes.c_int]),
+    ("gpupi_ntt_shape", ctypes.c_int, [_u32, _u32, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    ("gpupi_autotune", ctypes.c_int, [_p, ctypes.c_char_p, ctypes.c_uint64]),
     ("gpupi_decimal_naive", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32]),
     ("gpupi_convert_decimal", ctypes.c_int, [_p, _p, _u32, _u32, _u32, _u32, _p]),
     ("gpupi_pi_compute", ctypes.c_int,
@@ -263,6 +270,50 @@ def mul_tc(N, A, La, sA, B, Lb, sB, C, sC):
 def tc_error() -> int:
     """Device error word of the tensor-core kernels (read and cleared)."""
     return int(lib().gpupi_tc_error())
+
+
+MUL_KINDS = ("school", "tc", "ntt")
+TUNE_TABLE_PATH = _HERE / "tune_table.txt"
+
+
+def tune_load(path=None, text: str | None = None) -> int:
+    """Load a tune table from a file or from text (host only, no GPU needed);
+    returns the number of entries (raises on a malformed line)."""
+    n = lib().gpupi_tune_load_text(text.encode()) if text is not None else lib().gpupi_tune_load(str(path).encode())
+    if n < 0:
+        raise GpupiError(f"tune table: malformed line {-n}" if n > -1000000 else "tune table: cannot read file")
+    return n
+
+
+def tune_reset() -> None:
+    lib().gpupi_tune_reset()
+
+
+def tune_describe() -> str:
+    n = lib().gpupi_tune_describe(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib().gpupi_tune_describe(buf, n + 1)
+    return buf.value.decode()
+
+
+def mul_kind(La: int, Lb: int, public_api: bool = False) -> str:
+    """Kernel a product of La x Lb limbs uses under the table in effect."""
+    return MUL_KINDS[lib().gpupi_mul_kind(La, Lb, 1 if public_api else 0)]
+
+
+def ntt_shape(La: int, Lb: int) -> tuple[int, int]:
+    """(log_k, M): the NTT transform shape of an La x Lb product under the table in effect."""
+    lk, m = ctypes.c_int(0), ctypes.c_int(0)
+    _check(lib().gpupi_ntt_shape(La, Lb, ctypes.byref(lk), ctypes.byref(m)), "gpupi_ntt_shape")
+    return lk.value, m.value
+
+
+def autotune(ctx: "Context", path=TUNE_TABLE_PATH, budget_limbs: int = 1 << 24) -> str:
+    """Measure every candidate on the current GPU, write the table to `path`
+    and load it; returns the table text."""
+    _torch()
+    _check(lib().gpupi_autotune(ctx.h, str(path).encode(), budget_limbs), "gpupi_autotune")
+    return Path(path).read_text()
 
 
 def decimal_naive(N, A, L_limb, sA, out, L_dec, s_out):

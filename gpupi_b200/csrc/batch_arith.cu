@@ -161,16 +161,23 @@ size_t kernel_timer_report(char *buf, size_t cap) {
 void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La,
                 uint32_t Lb, uint64_t sA, uint64_t sB, uint64_t sC);
 bool school_thread_fits(uint32_t La, uint32_t Lb);
+cudaError_t tc_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La, uint32_t Lb,
+                   uint64_t sA, uint64_t sB, uint64_t sC);
+enum MulKind { kSchool = 0, kTensor = 1, kNtt = 2 };
+int mul_kind(uint32_t La, uint32_t Lb, bool public_api);   // tune.cu: school / tc / ntt per length bucket
+void tune_load_default();
 
 // Largest L_a + L_b handled by schoolbook.  The public batch_mp_mul keeps the
 // reference's rule (schoolbook up to 1024, batch_arith.cu:181: such products
-// never grow the context workspace, which gpupi's own tests check).  The
+// never grow the context workspace, which gpupi's own tests check), with the
+// tensor-core schoolbook where the tune table says it is faster.  The
 // library's own algorithms (pi pipeline, decimal conversion, ragged batches)
-// use mul_tuned: on B200 this library's NTT overtakes its schoolbook kernels
-// between 384 and 512 limbs (batched products of 2^27 limbs in total:
-// 384 -> 3.8 ms school / 4.7 ms NTT, 512 -> 4.6 / 3.7 ms), so its switch is at
-// 448.  The product is exact either way.  Overridable for tuning with
-// gpupi_set_mul_crossover().
+// use mul_tuned: the tune table's kernel per length bucket (tune.cu), else
+// the built-in rule: on B200 this library's NTT overtakes its CUDA-core
+// schoolbook between 384 and 512 limbs (batched products of 2^27 limbs in
+// total: 384 -> 3.8 ms school / 4.7 ms NTT, 512 -> 4.6 / 3.7 ms), so its
+// switch is at 448.  The product is exact either way.  The built-in switch is
+// overridable with gpupi_set_mul_crossover().
 constexpr uint32_t kRefSchoolMax = 1024u;
 static uint32_t g_school_max = 448u;
 
@@ -250,6 +257,7 @@ void batch_mp_array_release(BatchMPArray array) {
 }
 
 BatchMPContext *batch_mp_init() {
+    gpupi::tune_load_default();
     BatchMPContext *ctx = new (std::nothrow) BatchMPContext{};
     if (!ctx) return nullptr;
     if (allocate_tables(ctx) != cudaSuccess) {
@@ -282,15 +290,15 @@ static cudaError_t mul_with(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B,
     if (!same_batch(A, B) || !same_batch(A, C)) return cudaErrorInvalidValue;
     if ((uint64_t)C.length != (uint64_t)A.length + B.length) return cudaErrorInvalidValue;
     if (A.batch_size == 0u || C.length == 0u) return cudaSuccess;
-    const uint32_t L = A.length + B.length;
-    const bool school = A.length == 0u || B.length == 0u ||
-                        gpupi::school_thread_fits(A.length, B.length) ||
-                        (L <= school_max && L <= (uint32_t)BATCH_MUL_NAIVE_L_MAX);
-    if (school) {
+    const int kind = gpupi::mul_kind(A.length, B.length, school_max == kRefSchoolMax);
+    if (kind == gpupi::kSchool) {
         gpupi::school_mul(A.data, B.data, C.data, A.batch_size, A.length, B.length, A.stride, B.stride,
                           C.stride);
         return cudaGetLastError();
     }
+    if (kind == gpupi::kTensor)
+        return gpupi::tc_mul(A.data, B.data, C.data, A.batch_size, A.length, B.length, A.stride, B.stride,
+                             C.stride);
     cudaError_t err = ensure_workspace(ctx, batch_mul_ntt_workspace_size(A.batch_size, A.length, B.length));
     if (err != cudaSuccess) return err;
     batch_mul_ntt(A.data, B.data, C.data, ctx->workspace, ctx->ntt_tables, A.batch_size, A.length,

@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <string>
 
 struct gpupi_ctx {
     BatchMPContext *ctx;
@@ -24,6 +25,13 @@ cudaError_t tc_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N
                    uint64_t sA, uint64_t sB, uint64_t sC);
 bool tc_fits(uint32_t La, uint32_t Lb);
 uint32_t tc_error();
+int mul_kind(uint32_t La, uint32_t Lb, bool public_api);
+void ntt_shape_of(uint32_t La, uint32_t Lb, int *log_k, int *M);
+int tune_load(const char *path);
+int tune_load_text(const char *text);
+void tune_reset();
+std::string tune_describe();
+cudaError_t autotune(BatchMPContext *ctx, const char *path, uint64_t budget_limbs, std::string *report);
 cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const uint64_t *offA, const uint32_t *La,
                        const uint32_t *B, const uint64_t *offB, const uint32_t *Lb, uint32_t *C,
                        const uint64_t *offC);
@@ -175,6 +183,31 @@ int gpupi_mul_tc(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const 
 }
 
 int gpupi_tc_error(void) { return (int)gpupi::tc_error(); }
+
+int gpupi_tune_load(const char *path) { return gpupi::tune_load(path); }
+int gpupi_tune_load_text(const char *text) { return gpupi::tune_load_text(text); }
+int gpupi_tune_reset(void) {
+    gpupi::tune_reset();
+    return 0;
+}
+size_t gpupi_tune_describe(char *buf, size_t cap) {
+    const std::string s = gpupi::tune_describe();
+    if (buf && cap) {
+        const size_t n = std::min(cap - 1, s.size());
+        memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return s.size();
+}
+int gpupi_mul_kind(uint32_t La, uint32_t Lb, int public_api) { return gpupi::mul_kind(La, Lb, public_api != 0); }
+int gpupi_ntt_shape(uint32_t La, uint32_t Lb, int *log_k, int *M) {
+    if (!log_k || !M || La == 0u || Lb == 0u) return (int)cudaErrorInvalidValue;
+    gpupi::ntt_shape_of(La, Lb, log_k, M);
+    return 0;
+}
+int gpupi_autotune(gpupi_ctx *ctx, const char *path, uint64_t budget_limbs) {
+    return (int)gpupi::autotune(raw(ctx), path, budget_limbs, nullptr);
+}
 
 int gpupi_mp_mul_ragged(gpupi_ctx *ctx, uint32_t N, const uint32_t *A, const uint64_t *offA, const uint32_t *La,
                         const uint32_t *B, const uint64_t *offB, const uint32_t *Lb, uint32_t *C,

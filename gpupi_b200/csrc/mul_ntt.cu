@@ -893,6 +893,21 @@ struct Shape {
 
 // Smallest shape with M * K >= L_a + L_b - 1: one power-of-two transform up to
 // 2^25 points, above that M cosets of 2^25 points.
+}  // namespace ntt
+bool ntt_shape_override(uint64_t need, int *log_k, int *M);   // tune.cu
+namespace ntt {
+
+static Shape shape_for(uint32_t La, uint32_t Lb);
+
+// The product's transform shape: the tune table's, else the built-in rule
+// (shape_for).  Used by the plain product and its workspace size; the
+// tuned splitting tree's spectra keep the built-in rule.
+static Shape shape_tuned(uint32_t La, uint32_t Lb) {
+    int lk = 0, M = 0;
+    if (ntt_shape_override((uint64_t)La + Lb - 1u, &lk, &M)) return Shape{lk, M};
+    return shape_for(La, Lb);
+}
+
 static Shape shape_for(uint32_t La, uint32_t Lb) {
     const uint64_t need = (uint64_t)La + Lb - 1u;
     if (need <= (1ull << kMaxLog)) {
@@ -1091,7 +1106,7 @@ static void launch_combine(int M, const NttParams &P, const CombineArgs &c, uint
 
 size_t workspace_bytes(uint32_t N, uint32_t La, uint32_t Lb) {
     if (N == 0u || La == 0u || Lb == 0u) return 0;
-    const Shape s = shape_for(La, Lb);
+    const Shape s = shape_tuned(La, Lb);
     const uint64_t K = 1ull << s.log_k;
     const uint64_t Lc = (uint64_t)La + Lb;
     const uint64_t tiles = (Lc + kCrtSpan - 1) / kCrtSpan;
@@ -1107,7 +1122,7 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
         cudaMemset2DAsync(C, sC * 4, 0, (size_t)Lc * 4, N, st);
         return;
     }
-    const Shape s = shape_for(La, Lb);
+    const Shape s = shape_tuned(La, Lb);
     if (s.M > kMaxCosets) {
         fprintf(stderr, "gpupi_b200: product of %u limbs exceeds the 20 * 2^25-point limit\n", Lc);
         return;
@@ -1364,6 +1379,13 @@ size_t batch_mul_ntt_workspace_size(uint32_t N, uint32_t L_a, uint32_t L_b) {
 }
 
 namespace gpupi {
+
+// Transform shape a product of La x Lb limbs gets (tune table or built-in rule).
+void ntt_shape_of(uint32_t La, uint32_t Lb, int *log_k, int *M) {
+    const ntt::Shape s = ntt::shape_tuned(La, Lb);
+    *log_k = s.log_k;
+    *M = s.M;
+}
 
 SpectrumShape spectrum_shape(uint64_t ncoef) {
     if (ncoef < 2u || ncoef > ((uint64_t)ntt::kMaxCosets << ntt::kMaxLog)) return SpectrumShape{0, 0};

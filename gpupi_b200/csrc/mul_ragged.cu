@@ -4,8 +4,10 @@
 //
 // Products are bucketed on the host:
 //   * L_a = 0 or L_b = 0: the L_a + L_b output limbs are zeroed;
-//   * L_a + L_b <= the schoolbook crossover: one k_school_cols launch reading
-//     every product's offsets and lengths from a descriptor array;
+//   * products the tune table gives to the CUDA-core schoolbook: one
+//     k_school_cols launch reading every product's offsets and lengths from a
+//     descriptor array; those it gives to the tensor-core schoolbook: one
+//     k_mul_tc launch over their descriptors;
 //   * otherwise by transform size 2^ceil(log2(L_a + L_b - 1)): each bucket's
 //     operands are gathered into zero-padded rows (longer operand first: the
 //     product commutes), multiplied as one uniform batch (mul_tuned), and
@@ -24,7 +26,10 @@ namespace gpupi {
 
 void school_mul_ragged(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, const RaggedRow *rows,
                        uint64_t limb_products);
-uint32_t school_max();
+cudaError_t tc_mul_ragged(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t n, const RaggedRow *rows,
+                          uint32_t maxQ, uint32_t maxN, uint64_t limbs_moved);
+void tc_shape(uint32_t La, uint32_t Lb, uint32_t *Q, uint32_t *N);
+int mul_kind(uint32_t La, uint32_t Lb, bool public_api);
 cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 
 namespace {
@@ -140,26 +145,35 @@ cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const
     if (N == 0u) return cudaSuccess;
     if (!ctx || !A || !B || !C || !offA || !La || !offB || !Lb || !offC) return cudaErrorInvalidValue;
     cudaStream_t st = current_stream();
-    std::vector<RaggedRow> zero, school;
+    std::vector<RaggedRow> zero, school, tensor;
     std::map<int, std::vector<RaggedRow>> ntt;   // by log2 of the transform size
-    uint64_t school_work = 0;
+    uint64_t school_work = 0, tc_limbs = 0;
+    uint32_t tcQ = 0, tcN = 0;
     for (uint32_t i = 0; i < N; ++i) {
         const RaggedRow d{offA[i], offB[i], offC[i], La[i], Lb[i]};
         const uint64_t Lc = (uint64_t)d.La + d.Lb;
         if (Lc > (20ull << 25) || std::min(d.La, d.Lb) > (1u << 28)) return cudaErrorInvalidValue;
         if (d.La == 0u || d.Lb == 0u) {
             zero.push_back(d);
-        } else if (Lc <= school_max()) {
+        } else if (const int kind = mul_kind(d.La, d.Lb, false); kind == 0) {
             school.push_back(d);
             school_work += (uint64_t)d.La * d.Lb;
+        } else if (kind == 1) {
+            tensor.push_back(d);
+            uint32_t q = 0, n = 0;
+            tc_shape(d.La, d.Lb, &q, &n);
+            tcQ = std::max(tcQ, q);
+            tcN = std::max(tcN, n);
+            tc_limbs += 2ull * Lc;
         } else {
             ntt[ceil_log2_u64(Lc - 1)].push_back(d);
         }
     }
     cudaError_t err = cudaSuccess;
-    if (!zero.empty() || !school.empty()) {
+    if (!zero.empty() || !school.empty() || !tensor.empty()) {
         std::vector<RaggedRow> both(zero);
         both.insert(both.end(), school.begin(), school.end());
+        both.insert(both.end(), tensor.begin(), tensor.end());
         RaggedRow *dr = nullptr;
         err = scratch_alloc((void **)&dr, both.size() * sizeof(RaggedRow));
         if (err == cudaSuccess) {
@@ -172,6 +186,9 @@ cudaError_t mul_ragged(BatchMPContext *ctx, uint32_t N, const uint32_t *A, const
         }
         if (err == cudaSuccess && !school.empty())
             school_mul_ragged(A, B, C, (uint32_t)school.size(), dr + zero.size(), school_work);
+        if (err == cudaSuccess && !tensor.empty())
+            err = tc_mul_ragged(A, B, C, (uint32_t)tensor.size(), dr + zero.size() + school.size(), tcQ, tcN,
+                                tc_limbs);
         if (err == cudaSuccess) err = cudaGetLastError();
         scratch_free(dr);
     }

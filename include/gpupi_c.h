@@ -92,6 +92,33 @@ int gpupi_mul_tc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_
  * incomplete), 0 otherwise.  Synchronises with the device. */
 int gpupi_tc_error(void);
 
+/* Tune table (replaces the reference's compile-time BATCH_MUL_NAIVE_L_MAX,
+ * batch_arith.cu:181, get_N_max and the NTT schedule tables,
+ * batch_mul_ntt.cu:1781-1915): per length bucket, the product kernel
+ * (CUDA-core schoolbook, tensor-core schoolbook or NTT) and the NTT's
+ * transform shape (K points x M cosets).  Text lines
+ *     mul <max_sum> school|tc|ntt
+ *     ntt <min_need> <max_need> <log_k> <M>
+ * ('#' comments).  Read at context creation from $GPUPI_TUNE_TABLE, else
+ * tune_table.txt beside the library.  Results are bit-identical whatever the
+ * table says.  load / load_text return the number of entries, or
+ * -(line number) of the first malformed line (the table is then unchanged);
+ * reset returns to the built-in rule; describe writes the table in effect.
+ * gpupi_mul_kind: the kernel a product would use (0 schoolbook, 1 tensor
+ * cores, 2 NTT; public_api = gpupi's batch_mp_mul rule).  gpupi_autotune
+ * measures every candidate on the current GPU (batches of about
+ * budget_limbs operand limbs), checks each candidate's product word for
+ * word, writes the table to path and loads it. */
+int gpupi_tune_load(const char *path);
+int gpupi_tune_load_text(const char *text);
+int gpupi_tune_reset(void);
+size_t gpupi_tune_describe(char *buf, size_t cap);
+int gpupi_mul_kind(uint32_t L_a, uint32_t L_b, int public_api);
+/* Transform shape (2^log_k points x M cosets) of an NTT product of L_a x L_b
+ * limbs under the table in effect (host only). */
+int gpupi_ntt_shape(uint32_t L_a, uint32_t L_b, int *log_k, int *M);
+int gpupi_autotune(gpupi_ctx *ctx, const char *path, uint64_t budget_limbs);
+
 /* Ragged batch (no counterpart in the reference, whose batches share one
  * L_a / L_b): product i = A[offA[i] .. + L_a[i]) * B[offB[i] .. + L_b[i]) into
  * C[offC[i] .. + L_a[i] + L_b[i]).  d_A, d_B, d_C are device pointers; the
