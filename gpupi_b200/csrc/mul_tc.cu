@@ -31,7 +31,7 @@
 // Epilogue: D is read back with tcgen05.ld into shared memory, limb L of
 // the product is S_L = c_4L + c_(4L+1) 2^8 + c_(4L+2) 2^16 + c_(4L+3) 2^24
 // (< 2^56), and limb_L = lo(S_L) + hi(S_(L-1)) + carry, the binary carries
-// resolved with ballots across the CTA, pass after pass of 1024 limbs.
+// resolved with ballots across the CTA, pass after pass of 512 limbs.
 //
 // Limits: min(L_a, L_b) <= 2048, L_a + L_b <= 8192 (N <= 256 columns).
 // Waits on the MMA completion barrier are bounded; a wait that runs out sets
@@ -42,7 +42,7 @@
 namespace gpupi {
 namespace tc {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;   // four warps: one per tensor-memory lane quadrant
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kMaxShort = 2048u;   // limbs of the shorter operand
 constexpr uint32_t kMaxSum = 8192u;     // L_a + L_b
@@ -74,6 +74,11 @@ struct Layout {
 
 __host__ __device__ inline uint32_t up128(uint32_t x) { return (x + 127u) & ~127u; }
 
+// Rows per plane: N + Q - 1, rounded up to an odd count so that the eight
+// planes' rows u' fall in eight different 16-byte bank groups (the fill
+// writes one row of all eight planes per eight lanes).
+__host__ __device__ inline uint32_t plane_rows(uint32_t Q, uint32_t N) { return (N + Q - 1u) | 1u; }
+
 __host__ __device__ inline Layout layout_of(uint32_t maxQ, uint32_t maxN) {
     Layout l;
     l.abuf = 0u;
@@ -81,7 +86,7 @@ __host__ __device__ inline Layout layout_of(uint32_t maxQ, uint32_t maxN) {
     l.p = abytes;
     const uint32_t psz = 16u * (128u * maxQ + 112u), csz = 4u * 128u * maxN;
     l.planes = l.p + up128(psz > csz ? psz : csz);
-    l.total = l.planes + 8u * 16u * (maxN + maxQ - 1u);
+    l.total = l.planes + 8u * 16u * plane_rows(maxQ, maxN);
     return l;
 }
 
@@ -153,7 +158,7 @@ __device__ __forceinline__ uint64_t limb_sum(const uint32_t *cs, uint32_t L, uin
 }
 
 template <bool RAGGED>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 8)
     k_mul_tc(const uint32_t *__restrict__ A, const uint32_t *__restrict__ B, uint32_t *__restrict__ C, uint32_t nrows,
              uint32_t La_u, uint32_t Lb_u, uint64_t sA, uint64_t sB, uint64_t sC,
              const RaggedRow *__restrict__ rows, uint32_t tmem_cols, uint32_t maxQ, uint32_t maxN) {
@@ -195,15 +200,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         const Shape sh = shape_of(La, Lb);
         const uint32_t prow_n = 128u * sh.Q + 112u;    // rows of P
         const uint32_t brow_n = sh.N + sh.Q - 1u;      // rows of each plane
-        const uint32_t plane_bytes = 16u * brow_n;
+        const uint32_t plane_bytes = 16u * plane_rows(sh.Q, sh.N);
 
         // 1. a's limbs at byte 128 of abuf (limb w - 32 in word w), zeros around
         const uint32_t abw = (128u * sh.Q + 160u) / 4u;
         for (uint32_t w = tid; w < abw; w += kThreads) abuf[w] = (w >= 32u && w - 32u < La) ? ap[w - 32u] : 0u;
         // 2. the planes of b: plane j row rr holds b[128u' + 16(7-j) .. +16)
-        //    reversed, u' = rr - (Q - 1); zero outside b
+        //    reversed, u' = rr - (Q - 1); zero outside b.  Eight consecutive
+        //    threads read one 128-byte block of b (coalesced) and write row
+        //    rr of the eight planes.
         for (uint32_t idx = tid; idx < 8u * brow_n; idx += kThreads) {
-            const uint32_t j = idx / brow_n, rr = idx - j * brow_n;
+            const uint32_t j = idx & 7u, rr = idx >> 3;
             const int up = (int)rr - (int)(sh.Q - 1u);
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (up >= 0) {
@@ -268,13 +275,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         fence_after();
         // 6. D -> shared memory: cs[128u + s] = c_(128u + s) (the MMAs no
-        //    longer read P, whose space this reuses)
+        //    longer read P, whose space this reuses); warp w reads lanes
+        //    32w .. 32w + 31 of tensor memory
         {
-            const uint32_t qd = warp & 3u, half = warp >> 2;
-            const uint32_t s = 32u * qd + lane;
-            for (uint32_t g = half; g < sh.N / 16u; g += 2u) {
+            const uint32_t s = 32u * warp + lane;
+            for (uint32_t g = 0; g < sh.N / 16u; ++g) {
                 uint32_t r[16];
-                tmem_ld16(tmem + ((32u * qd) << 16) + 16u * g, r);
+                tmem_ld16(tmem + ((32u * warp) << 16) + 16u * g, r);
 #pragma unroll
                 for (int e = 0; e < 16; ++e) cs[128u * (16u * g + e) + s] = r[e];
             }
@@ -355,11 +362,34 @@ cudaError_t launch_tc(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_
         if (err != cudaSuccess) return err;
         configured[RAGGED] = smem;
     }
-    // CTAs per SM: shared memory allows `occ`; tensor memory allows 512 / cols
-    int occ = 1;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tc::k_mul_tc<RAGGED>, tc::kThreads, smem);
-    if (err != cudaSuccess) return err;
-    occ = std::max(1, std::min(occ, (int)(512u / cols)));
+    // Resident CTAs per SM, the grid of this persistent kernel: the least of
+    // what threads, registers (allocated per warp in units of 256),
+    // shared memory (plus the 1 KiB the driver reserves per CTA) and
+    // tensor memory (512 columns per SM) allow.  More CTAs than that would
+    // only wait in tcgen05.alloc for a resident one to finish.
+    static int occ_cache[2][6] = {};   // by RAGGED and log2(cols / 32)
+    int lc = 0;
+    while ((32u << lc) < cols) ++lc;
+    int &occ = occ_cache[RAGGED][lc];
+    static size_t occ_smem[2][6] = {};
+    if (occ == 0 || occ_smem[RAGGED][lc] != smem) {
+        cudaFuncAttributes fa{};
+        err = cudaFuncGetAttributes(&fa, tc::k_mul_tc<RAGGED>);
+        if (err != cudaSuccess) return err;
+        int dev = 0, smem_sm = 0, regs_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        const int warps = tc::kThreads / 32;
+        const int regs_cta = warps * ((fa.numRegs * 32 + 255) / 256) * 256;
+        const size_t smem_cta = smem + fa.sharedSizeBytes + 1024u;
+        int o = 2048 / tc::kThreads;
+        o = std::min(o, regs_sm / std::max(regs_cta, 1));
+        o = std::min(o, (int)((size_t)smem_sm / smem_cta));
+        o = std::min(o, (int)(512u / cols));
+        occ = std::max(o, 1);
+        occ_smem[RAGGED][lc] = smem;
+    }
     const unsigned grid = (unsigned)std::min<uint64_t>(n, (uint64_t)kNumSMs * occ);
     tc::k_mul_tc<RAGGED><<<grid, tc::kThreads, smem, st>>>(A, B, C, n, La, Lb, sA, sB, sC, rows, cols, maxQ, maxN);
     count_launch();
