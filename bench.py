@@ -62,6 +62,21 @@ NCU_TRAFFIC_SOURCE = {"ntt_rows_fused": "ncu capture of k_rows_r<12> on a 2^22 x
                                             "product, scaled to each launch by its algorithmic bytes",
                       "ntt_rows_level": "ncu capture of k_rows_level in pi to 1e8 digits (2^25 points x 3 primes "
                                         "per launch), scaled to each launch by its algorithmic bytes"}
+# Warp instructions per algorithmic byte of each kernel family, by pipe
+# (FMA-heavy = IMAD, ALU, all), from one ncu capture of every launch of pi to
+# 1e8 digits with the library's kernel-timer bytes of the same computation
+# (profiles/int_pipes_pi1e8.md).  Scaled to this run's bytes and divided by
+# the live integer-pipe peaks they give each family's integer roofline.
+INT_WINST_PER_BYTE = {
+    "ntt_rows_level": (0.197852, 0.203125, 0.47631), "ntt_cols_fwd_first": (0.191449, 0.215956, 0.487502),
+    "ntt_cols_inv": (0.100019, 0.111781, 0.246528), "ntt_rows_fused": (0.223939, 0.221069, 0.529707),
+    "schoolbook_tc": (0.140841, 0.26468, 0.758519), "ntt_crt_carry": (0.075807, 0.089089, 0.220724),
+    "carry_chain": (0.078094, 0.116731, 0.274415), "schoolbook": (0.252166, 0.182724, 0.584128),
+    "ntt_cols_fwd": (0.078664, 0.093384, 0.199631), "ntt_local": (0.55531, 0.538007, 1.292256),
+    "ntt_coset_combine": (0.10361, 0.100811, 0.266338), "decimal_extract": (0.075693, 0.08626, 0.224201),
+    "decimal_leaf": (0.596097, 0.168555, 0.837855), "shift": (0.035647, 0.045182, 0.115069)}
+INT_SOURCE = ("ncu sm__inst_executed_pipe_{fmaheavy,alu}.sum and sm__inst_executed.sum over every launch of "
+              "pi_bs_gpu 100000000 (profiles/int_pipes_pi1e8.md), per algorithmic byte, scaled to this run")
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ms to 1e9 digits of pi (bit-exact), tuned vs plain form on B200; NTT HBM GB/s"
@@ -450,6 +465,29 @@ def run_ours(args, ws, rank, local):
                 "peak_source": "measured" if not peaks.get("fallback") else "fallback"}
     families = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
                     "GBps": (v[2] / (v[1] * 1e-3) / 1e9) if v[1] > 0 else None} for k, v in ktimes.items()}
+    # integer roofline of each family: t_min = max(IMAD / IMAD peak, ALU /
+    # ALU peak, all / issue peak) from the instruction counts per byte
+    ipk = g.int_peak()
+    pim, pal = ipk["imad_winst_per_s"], ipk["alu_winst_per_s"]
+    for k, f in families.items():
+        r = INT_WINST_PER_BYTE.get(k)
+        n, kms, kbytes = ktimes[k]
+        if r and kms > 0:
+            tmin = max(r[0] * kbytes / pim, r[1] * kbytes / pal, r[2] * kbytes / (pim + pal))
+            f["int_roofline_frac"] = tmin / (kms * 1e-3)
+    roof_int = None
+    if dom and dom[0] in INT_WINST_PER_BYTE:
+        name, (n, kms, kbytes) = dom
+        r = INT_WINST_PER_BYTE[name]
+        achieved = r[2] * kbytes / (kms * 1e-3)
+        roof_int = {"bound": "integer issue", "kernel": name, "achieved": achieved, "peak": pim + pal,
+                    "unit": "warp instructions/s", "frac": families[name]["int_roofline_frac"],
+                    "imad_pipe_frac": r[0] * kbytes / (kms * 1e-3) / pim,
+                    "alu_pipe_frac": r[1] * kbytes / (kms * 1e-3) / pal,
+                    "peaks_measured": {"imad_winst_per_s": pim, "alu_winst_per_s": pal,
+                                       "how": "gpupi_int_peak (csrc/int_peak.cu) in this run"},
+                    "source": INT_SOURCE,
+                    "note": "the binding roofline of the NTT passes; roofline (HBM) above is the contract's"}
 
     if rank != 0:
         return
@@ -493,6 +531,7 @@ def run_ours(args, ws, rank, local):
                 "d2h_bytes_per_step": (d1 - d0) // args.steps},
         "gpu_launches": launches,
         "roofline": roof,
+        "roofline_int": roof_int,
         "kernel_families": families,
         "launch_gaps": {
             "device_ms_per_step": sum(v[1] for v in kgaps.values()) / args.steps,
@@ -590,6 +629,20 @@ def run_convert(args, ws, rank, local):
     ctx.close()
 
 
+def run_intpeak(args, ws, rank, local):
+    """The integer-pipe peaks every limb kernel is measured against."""
+    import torch
+    import gpupi_b200 as g
+    torch.cuda.set_device(local)
+    runs = [g.int_peak() for _ in range(max(1, args.steps))]
+    best = {k: max(r[k] for r in runs) for k in runs[0]}
+    if rank == 0:
+        print(json.dumps({"metric": "integer-pipe peak (warp instructions per second)", "value": best["imad_winst_per_s"],
+                          "unit": "warp IMAD/s", "alu_winst_per_s": best["alu_winst_per_s"], "steps": len(runs),
+                          "how": "eight independent mad.lo.u32 (lop3.b32) chains per thread, 2 x 1024 threads "
+                                 "per SM, CUDA events (csrc/int_peak.cu)"}), flush=True)
+
+
 def run_uneven(args, ws, rank, local):
     """4096 independent products with lengths log-uniform in [8, 4096] limbs
     per operand (seeded), operands resident in HBM: one ragged call
@@ -658,9 +711,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--digits", type=int, default=1_000_000_000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", choices=["pi", "ntt", "convert", "uneven"], default="pi",
+    ap.add_argument("--workload", choices=["pi", "ntt", "convert", "uneven", "intpeak"], default="pi",
                     help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step; "
-                         "convert: one 2^25-limb decimal conversion per step; uneven: 4096 uneven products")
+                         "convert: one 2^25-limb decimal conversion per step; uneven: 4096 uneven products; "
+                         "intpeak: the integer-pipe peaks")
     ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
     ap.add_argument("--ntt-path", choices=["fused", "spectra"], default="fused",
                     help="ntt workload: fused row pass, or forward / inverse spectra")
@@ -691,6 +745,8 @@ def main():
             run_convert(args, ws, rank, local)
         elif args.workload == "uneven":
             run_uneven(args, ws, rank, local)
+        elif args.workload == "intpeak":
+            run_intpeak(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
         ok = True

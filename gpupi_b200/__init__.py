@@ -55,6 +55,7 @@ _SIGS = [
     ("gpupi_mul_ntt", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_mul_tc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_tc_error", ctypes.c_int, []),
+    ("gpupi_int_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("gpupi_tune_load", ctypes.c_int, [ctypes.c_char_p]),
     ("gpupi_tune_load_text", ctypes.c_int, [ctypes.c_char_p]),
     ("gpupi_tune_reset", ctypes.c_int, []),
@@ -270,6 +271,14 @@ def mul_tc(N, A, La, sA, B, Lb, sB, C, sC):
 def tc_error() -> int:
     """Device error word of the tensor-core kernels (read and cleared)."""
     return int(lib().gpupi_tc_error())
+
+
+def int_peak() -> dict:
+    """Measured integer-pipe peaks (warp instructions per second)."""
+    _torch()
+    a, b = ctypes.c_double(0), ctypes.c_double(0)
+    _check(lib().gpupi_int_peak(ctypes.byref(a), ctypes.byref(b)), "gpupi_int_peak")
+    return {"imad_winst_per_s": a.value, "alu_winst_per_s": b.value}
 
 
 MUL_KINDS = ("school", "tc", "ntt")

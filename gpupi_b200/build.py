@@ -31,7 +31,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 
 LIB_SOURCES = [
     "batch_arith.cu", "carry_ops.cu", "shift.cu", "bitlength.cu", "exactdiv.cu",
-    "mul_naive.cu", "mul_tc.cu", "mul_ntt.cu", "decimal.cu", "pi_engine.cu", "bbp.cu", "mul_ragged.cu", "scratch.cu", "tune.cu", "capi.cu",
+    "mul_naive.cu", "mul_tc.cu", "mul_ntt.cu", "decimal.cu", "pi_engine.cu", "bbp.cu", "mul_ragged.cu", "scratch.cu", "tune.cu", "int_peak.cu", "capi.cu",
 ]
 CLI_SOURCES = ["pi_main.cu"]
 

@@ -26,6 +26,7 @@ cudaError_t tc_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N
 bool tc_fits(uint32_t La, uint32_t Lb);
 uint32_t tc_error();
 int mul_kind(uint32_t La, uint32_t Lb, bool public_api);
+cudaError_t int_peak(double *imad_winst_per_s, double *alu_winst_per_s);
 void ntt_shape_of(uint32_t La, uint32_t Lb, int *log_k, int *M);
 int tune_load(const char *path);
 int tune_load_text(const char *text);
@@ -183,6 +184,10 @@ int gpupi_mul_tc(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const 
 }
 
 int gpupi_tc_error(void) { return (int)gpupi::tc_error(); }
+
+int gpupi_int_peak(double *imad_winst_per_s, double *alu_winst_per_s) {
+    return (int)gpupi::int_peak(imad_winst_per_s, alu_winst_per_s);
+}
 
 int gpupi_tune_load(const char *path) { return gpupi::tune_load(path); }
 int gpupi_tune_load_text(const char *text) { return gpupi::tune_load_text(text); }

@@ -92,6 +92,13 @@ int gpupi_mul_tc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_
  * incomplete), 0 otherwise.  Synchronises with the device. */
 int gpupi_tc_error(void);
 
+/* Integer-pipe peaks of the current GPU (no counterpart in the reference):
+ * warp instructions per second of 32-bit multiply-adds (IMAD, the
+ * FMA-heavy pipe) and of three-input logic (LOP3, the ALU pipe), from
+ * eight independent chains per thread on every SM, timed with CUDA events.
+ * The ceiling the NTT and schoolbook kernels are measured against. */
+int gpupi_int_peak(double *imad_winst_per_s, double *alu_winst_per_s);
+
 /* Tune table (replaces the reference's compile-time BATCH_MUL_NAIVE_L_MAX,
  * batch_arith.cu:181, get_N_max and the NTT schedule tables,
  * batch_mul_ntt.cu:1781-1915): per length bucket, the product kernel
