@@ -470,20 +470,20 @@ def run_ours(args, ws, rank, local):
     ipk = g.int_peak()
     pim, pal = ipk["imad_winst_per_s"], ipk["alu_winst_per_s"]
     for k, f in families.items():
-        r = INT_WINST_PER_BYTE.get(k)
+        ir = INT_WINST_PER_BYTE.get(k)
         n, kms, kbytes = ktimes[k]
-        if r and kms > 0:
-            tmin = max(r[0] * kbytes / pim, r[1] * kbytes / pal, r[2] * kbytes / (pim + pal))
+        if ir and kms > 0:
+            tmin = max(ir[0] * kbytes / pim, ir[1] * kbytes / pal, ir[2] * kbytes / (pim + pal))
             f["int_roofline_frac"] = tmin / (kms * 1e-3)
     roof_int = None
     if dom and dom[0] in INT_WINST_PER_BYTE:
         name, (n, kms, kbytes) = dom
-        r = INT_WINST_PER_BYTE[name]
-        achieved = r[2] * kbytes / (kms * 1e-3)
+        ir = INT_WINST_PER_BYTE[name]
+        achieved = ir[2] * kbytes / (kms * 1e-3)
         roof_int = {"bound": "integer issue", "kernel": name, "achieved": achieved, "peak": pim + pal,
                     "unit": "warp instructions/s", "frac": families[name]["int_roofline_frac"],
-                    "imad_pipe_frac": r[0] * kbytes / (kms * 1e-3) / pim,
-                    "alu_pipe_frac": r[1] * kbytes / (kms * 1e-3) / pal,
+                    "imad_pipe_frac": ir[0] * kbytes / (kms * 1e-3) / pim,
+                    "alu_pipe_frac": ir[1] * kbytes / (kms * 1e-3) / pal,
                     "peaks_measured": {"imad_winst_per_s": pim, "alu_winst_per_s": pal,
                                        "how": "gpupi_int_peak (csrc/int_peak.cu) in this run"},
                     "source": INT_SOURCE,

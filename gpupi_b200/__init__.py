@@ -55,7 +55,10 @@ _SIGS = [
     ("gpupi_mul_ntt", ctypes.c_int, [_p, _u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_mul_tc", ctypes.c_int, [_u32, _p, _u32, _u32, _p, _u32, _u32, _p, _u32]),
     ("gpupi_tc_error", ctypes.c_int, []),
+    ("gpupi_tc_selftest_timeout", ctypes.c_int, [ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     ("gpupi_int_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("gpupi_fail_alloc", ctypes.c_int, [_u32, _u32]),
+    ("gpupi_scratch_live_bytes", ctypes.c_uint64, []),
     ("gpupi_tune_load", ctypes.c_int, [ctypes.c_char_p]),
     ("gpupi_tune_load_text", ctypes.c_int, [ctypes.c_char_p]),
     ("gpupi_tune_reset", ctypes.c_int, []),
@@ -281,6 +284,19 @@ def int_peak() -> dict:
     return {"imad_winst_per_s": a.value, "alu_winst_per_s": b.value}
 
 
+ALLOC_SCRATCH, ALLOC_WORKSPACE, ALLOC_ARRAY = 1, 2, 4
+
+
+def fail_alloc(kind_mask: int, nth: int) -> None:
+    """Make the nth following device allocation of a category in kind_mask
+    fail once (host-side injection for error-path tests; 0 disarms)."""
+    lib().gpupi_fail_alloc(kind_mask, nth)
+
+
+def scratch_live_bytes() -> int:
+    return int(lib().gpupi_scratch_live_bytes())
+
+
 MUL_KINDS = ("school", "tc", "ntt")
 TUNE_TABLE_PATH = _HERE / "tune_table.txt"
 
@@ -323,6 +339,14 @@ def autotune(ctx: "Context", path=TUNE_TABLE_PATH, budget_limbs: int = 1 << 24) 
     _torch()
     _check(lib().gpupi_autotune(ctx.h, str(path).encode(), budget_limbs), "gpupi_autotune")
     return Path(path).read_text()
+
+
+def tc_selftest_timeout() -> tuple[int, int]:
+    """(error word of the forced-timeout call, error word of a normal call after it)."""
+    _torch()
+    a, b = _u32(0), _u32(0)
+    _check(lib().gpupi_tc_selftest_timeout(ctypes.byref(a), ctypes.byref(b)), "gpupi_tc_selftest_timeout")
+    return a.value, b.value
 
 
 def decimal_naive(N, A, L_limb, sA, out, L_dec, s_out):

@@ -210,6 +210,7 @@ cudaError_t ensure_workspace(BatchMPContext *ctx, size_t bytes) {
     // the old buffer may still be in use by queued work
     cudaError_t err = cudaStreamSynchronize(gpupi::current_stream());
     if (err != cudaSuccess) return err;
+    if (gpupi::fail_alloc_now(gpupi::kAllocWorkspace)) return cudaErrorMemoryAllocation;
     err = cudaMalloc(&p, bytes);
     if (err != cudaSuccess) return err;
     if (ctx->workspace) cudaFree(ctx->workspace);
@@ -248,7 +249,7 @@ BatchMPArray batch_mp_array_create(uint32_t batch_size, uint32_t length, uint32_
     if (a.length > a.stride) return BatchMPArray{};
     const size_t bytes = (size_t)a.batch_size * a.stride * sizeof(uint32_t);
     if (bytes == 0u) return a;
-    if (cudaMalloc(&a.data, bytes) != cudaSuccess) a = BatchMPArray{};
+    if (gpupi::fail_alloc_now(gpupi::kAllocArray) || cudaMalloc(&a.data, bytes) != cudaSuccess) a = BatchMPArray{};
     return a;
 }
 

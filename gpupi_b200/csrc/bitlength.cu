@@ -1,8 +1,8 @@
 // Largest used bit / limb length over a batch (gpupi batch_bitlength.cu:33-245).
 //
 // Long rows (unless there are very many): 4096-limb chunks scanned from the
-// top by all CTAs, skipping chunks that cannot beat the best length found so
-// far.  Short rows, or very many rows: one thread per row, bounded by the
+// top by all CTAs; a CTA stops at the first chunk that cannot beat the best
+// length found so far (every later chunk of its sequence lies lower).  Short rows, or very many rows: one thread per row, bounded by the
 // best length seen so far.  Per-CTA maxima meet in one device word; the
 // last CTA to finish (ticket counter) moves the result straight into pinned,
 // mapped host memory and re-zeroes the word and the counter, so a call is one
@@ -44,7 +44,10 @@ __global__ void __launch_bounds__(256) length_max_chunks_kernel(const uint32_t *
             cta_max = 0u;
         }
         __syncthreads();
-        if (!skip) {
+        // items run top chunk first (chunk index major): once a chunk cannot
+        // beat the best length, no later item of this CTA can either
+        if (skip) break;
+        {
             const uint32_t *a = A + row * stride;
             uint32_t best = 0u;
 #pragma unroll 4

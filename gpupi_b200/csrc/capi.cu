@@ -25,6 +25,7 @@ cudaError_t tc_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N
                    uint64_t sA, uint64_t sB, uint64_t sC);
 bool tc_fits(uint32_t La, uint32_t Lb);
 uint32_t tc_error();
+cudaError_t tc_selftest_timeout(uint32_t *seen, uint32_t *after);
 int mul_kind(uint32_t La, uint32_t Lb, bool public_api);
 cudaError_t int_peak(double *imad_winst_per_s, double *alu_winst_per_s);
 void ntt_shape_of(uint32_t La, uint32_t Lb, int *log_k, int *M);
@@ -184,6 +185,18 @@ int gpupi_mul_tc(uint32_t N, const uint32_t *A, uint32_t La, uint32_t sA, const 
 }
 
 int gpupi_tc_error(void) { return (int)gpupi::tc_error(); }
+
+int gpupi_tc_selftest_timeout(uint32_t *seen, uint32_t *after) {
+    if (!seen || !after) return (int)cudaErrorInvalidValue;
+    return (int)gpupi::tc_selftest_timeout(seen, after);
+}
+
+int gpupi_fail_alloc(uint32_t kind_mask, uint32_t nth) {
+    gpupi::fail_alloc_arm(kind_mask, nth);
+    return 0;
+}
+
+uint64_t gpupi_scratch_live_bytes(void) { return gpupi::scratch_live_bytes(); }
 
 int gpupi_int_peak(double *imad_winst_per_s, double *alu_winst_per_s) {
     return (int)gpupi::int_peak(imad_winst_per_s, alu_winst_per_s);

@@ -48,6 +48,19 @@ void scratch_reserve(size_t bytes);   // grow the idle arena of the current stre
 void scratch_context_opened();
 void scratch_context_closed();
 void scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills);
+uint64_t scratch_live_bytes();
+
+// Host-side allocation-failure injection (tests of the error paths; no GPU
+// fault is involved): fail_alloc_arm(mask, n) makes the n-th following
+// device allocation whose category is in mask return
+// cudaErrorMemoryAllocation, once, without allocating.  Categories:
+enum AllocKind : uint32_t {
+    kAllocScratch = 1u,     // scratch arena requests (scratch_alloc)
+    kAllocWorkspace = 2u,   // growth of a context's workspace
+    kAllocArray = 4u,       // batch_mp_array_create
+};
+void fail_alloc_arm(uint32_t mask, uint32_t nth);
+bool fail_alloc_now(AllocKind kind);   // true: this allocation must fail
 
 // Optional per-kernel timing: when enabled, the launch sites bracket each
 // launch with CUDA events on the current stream and record the launch's

@@ -149,6 +149,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 constexpr uint32_t kWaitLimit = 1u << 22;   // polls of the completion barrier
+constexpr uint32_t kProbeLimit = 1u << 12;  // polls of the self-test's never-completing barrier
 
 // S_L = c_4L + c_(4L+1) 2^8 + c_(4L+2) 2^16 + c_(4L+3) 2^24 (0 beyond the product)
 __device__ __forceinline__ uint64_t limb_sum(const uint32_t *cs, uint32_t L, uint32_t Lc) {
@@ -161,9 +162,11 @@ template <bool RAGGED>
 __global__ void __launch_bounds__(kThreads, 8)
     k_mul_tc(const uint32_t *__restrict__ A, const uint32_t *__restrict__ B, uint32_t *__restrict__ C, uint32_t nrows,
              uint32_t La_u, uint32_t Lb_u, uint64_t sA, uint64_t sB, uint64_t sC,
-             const RaggedRow *__restrict__ rows, uint32_t tmem_cols, uint32_t maxQ, uint32_t maxN) {
+             const RaggedRow *__restrict__ rows, uint32_t tmem_cols, uint32_t maxQ, uint32_t maxN,
+             uint32_t probe_timeout) {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t mbar_never;   // no arrival ever: the timeout self-test waits on it
     __shared__ uint32_t tmem_slot;
     __shared__ uint32_t sg[kWarps], sp[kWarps];
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(kThreads, 8)
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar_never)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fence_before();
@@ -259,10 +263,21 @@ __global__ void __launch_bounds__(kThreads, 8)
             }
             mma_commit(mbar_a);
         }
-        // 5. bounded wait for the MMAs
+        // 5. bounded wait for the MMAs.  The timeout self-test first waits on
+        //    a barrier nothing arrives on, records that the wait ran out
+        //    (error word 2), then waits, bounded again, for its own MMAs so
+        //    that tensor memory is idle before it is released.
         uint32_t polls = 0u;
+        if (probe_timeout) {
+            while (!mbar_try_wait(smem_addr(&mbar_never), 0u) && ++polls < kProbeLimit) {
+            }
+            if (polls >= kProbeLimit && tid == 0) atomicExch(&g_tc_error, 2u);
+            failed = true;
+            polls = 0u;
+        }
         while (!mbar_try_wait(mbar_a, phase)) {
             if (++polls >= kWaitLimit) {
+                if (tid == 0) atomicExch(&g_tc_error, 1u);
                 failed = true;
                 break;
             }
@@ -270,7 +285,6 @@ __global__ void __launch_bounds__(kThreads, 8)
         phase ^= 1u;
         if (__syncthreads_or(failed)) {
             failed = true;
-            if (tid == 0) atomicExch(&g_tc_error, 1u);
             break;
         }
         fence_after();
@@ -342,7 +356,7 @@ uint32_t tmem_cols_for(uint32_t N) {
 template <bool RAGGED>
 cudaError_t launch_tc(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t n, uint32_t La, uint32_t Lb,
                       uint64_t sA, uint64_t sB, uint64_t sC, const RaggedRow *rows, uint32_t maxQ, uint32_t maxN,
-                      cudaStream_t st) {
+                      cudaStream_t st, uint32_t probe = 0u) {
     const tc::Layout lay = tc::layout_of(maxQ, maxN);
     const uint32_t cols = tmem_cols_for(maxN);
     // opt in to the dynamic shared memory this shape needs (once per size
@@ -391,7 +405,8 @@ cudaError_t launch_tc(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_
         occ_smem[RAGGED][lc] = smem;
     }
     const unsigned grid = (unsigned)std::min<uint64_t>(n, (uint64_t)kNumSMs * occ);
-    tc::k_mul_tc<RAGGED><<<grid, tc::kThreads, smem, st>>>(A, B, C, n, La, Lb, sA, sB, sC, rows, cols, maxQ, maxN);
+    tc::k_mul_tc<RAGGED><<<grid, tc::kThreads, smem, st>>>(A, B, C, n, La, Lb, sA, sB, sC, rows, cols, maxQ, maxN,
+                                                           probe);
     count_launch();
     return cudaGetLastError();
 }
@@ -419,6 +434,31 @@ void tc_shape(uint32_t La, uint32_t Lb, uint32_t *Q, uint32_t *N) {
     const tc::Shape sh = tc::shape_of(std::min(La, Lb), std::max(La, Lb));
     *Q = sh.Q;
     *N = sh.N;
+}
+
+uint32_t tc_error();
+
+// Timeout self-test: one 64 x 64-limb product whose CTA first waits on a
+// barrier that never completes.  Returns the error word that call left (2:
+// the bounded wait ran out and the kernel returned; the GPU stays usable)
+// and, in *after, the error word of an ordinary product right after it (0).
+cudaError_t tc_selftest_timeout(uint32_t *seen, uint32_t *after) {
+    uint32_t *buf = nullptr;
+    cudaError_t err = scratch_alloc((void **)&buf, 4u * 256u);
+    if (err != cudaSuccess) return err;
+    cudaStream_t st = current_stream();
+    cudaMemsetAsync(buf, 0x5a, 4u * 256u, st);
+    const tc::Shape sh = tc::shape_of(64u, 64u);
+    tc_error();
+    err = launch_tc<false>(buf, buf + 64, buf + 128, 1u, 64u, 64u, 64u, 64u, 128u, nullptr, sh.Q, sh.N, st, 1u);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err == cudaSuccess) *seen = tc_error();
+    if (err == cudaSuccess) err = launch_tc<false>(buf, buf + 64, buf + 128, 1u, 64u, 64u, 64u, 64u, 128u, nullptr,
+                                                   sh.Q, sh.N, st, 0u);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err == cudaSuccess) *after = tc_error();
+    scratch_free(buf);
+    return err;
 }
 
 // Reads and clears the device error word (1: a completion wait ran out).

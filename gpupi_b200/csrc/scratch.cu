@@ -142,8 +142,28 @@ Registry &registry() {
 
 }  // namespace
 
+namespace {
+std::mutex g_fail_mu;
+uint32_t g_fail_mask = 0u, g_fail_left = 0u;
+}  // namespace
+
+void fail_alloc_arm(uint32_t mask, uint32_t nth) {
+    std::lock_guard<std::mutex> g(g_fail_mu);
+    g_fail_mask = nth ? mask : 0u;
+    g_fail_left = nth;
+}
+
+bool fail_alloc_now(AllocKind kind) {
+    std::lock_guard<std::mutex> g(g_fail_mu);
+    if (!(g_fail_mask & kind) || g_fail_left == 0u) return false;
+    if (--g_fail_left != 0u) return false;
+    g_fail_mask = 0u;
+    return true;
+}
+
 cudaError_t scratch_alloc(void **p, size_t bytes) {
     if (!p) return cudaErrorInvalidValue;
+    if (fail_alloc_now(kAllocScratch)) return cudaErrorMemoryAllocation;
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
@@ -195,6 +215,14 @@ void scratch_context_closed() {
     }
     cudaSetDevice(cur);
     r.arenas.clear();
+}
+
+uint64_t scratch_live_bytes() {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    uint64_t live = 0;
+    for (auto &kv : r.arenas) live += kv.second.live_bytes;
+    return live;
 }
 
 void scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills) {

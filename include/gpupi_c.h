@@ -91,6 +91,24 @@ int gpupi_mul_tc(uint32_t N, const uint32_t *d_A, uint32_t L_a, uint32_t stride_
  * bounded wait for MMA completion ran out (the products are then
  * incomplete), 0 otherwise.  Synchronises with the device. */
 int gpupi_tc_error(void);
+/* Failure-detection self-test of the tensor-core kernel (no counterpart in
+ * the reference): one small product whose CTA first waits on a barrier that
+ * never completes.  The bounded wait runs out, the kernel records it
+ * (*seen = 2), waits for its own MMAs, frees its tensor memory and returns;
+ * an ordinary product right after it then leaves *after = 0 (the GPU and the
+ * context stay usable).  No GPU fault is involved. */
+int gpupi_tc_selftest_timeout(uint32_t *seen, uint32_t *after);
+
+/* Error-path testing (no counterpart in the reference, whose allocations
+ * are partly unchecked, pi_bs_gpu.cu:1199-1203): the nth following device
+ * allocation whose category is in kind_mask fails once with
+ * cudaErrorMemoryAllocation (returned as 2), on the host, without touching
+ * the GPU.  Categories: 1 scratch arena, 2 context workspace growth,
+ * 4 batch_mp_array_create.  nth = 0 disarms.  gpupi_scratch_live_bytes:
+ * bytes of the scratch arenas currently handed out (0 when no call is in
+ * progress and nothing leaked). */
+int gpupi_fail_alloc(uint32_t kind_mask, uint32_t nth);
+uint64_t gpupi_scratch_live_bytes(void);
 
 /* Integer-pipe peaks of the current GPU (no counterpart in the reference):
  * warp instructions per second of 32-bit multiply-adds (IMAD, the
