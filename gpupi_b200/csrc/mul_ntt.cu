@@ -686,6 +686,15 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
         run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
         store(F0, x);
     };
+    // The six operand segments (16 KiB each, contiguous, 16-byte aligned) go
+    // to L2 by bulk prefetch (the copy engine, no registers or shared memory)
+    // as the CTA starts, so the later loads, issued between transforms, find
+    // them in L2 instead of waiting on HBM.
+    if (t < 6u) {
+        const uint32_t *F = t == 0u ? a.Fpe : t == 1u ? a.Fpo : t == 2u ? a.Fro : t == 3u ? a.Fqo
+                                                                      : t == 4u ? a.Fqe : a.Fre;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F + off), "r"((uint32_t)C * 4u) : "memory");
+    }
     half(a.Fpe, a.Fpo, a.Fro);
     half(a.Fqo, a.Fqe, a.Fre);
 }
