@@ -643,6 +643,50 @@ def run_intpeak(args, ws, rank, local):
                                  "per SM, CUDA events (csrc/int_peak.cu)"}), flush=True)
 
 
+def run_mulsmall(args, ws, rank, local):
+    """One batch of equal products through each product kernel: the
+    CUDA-core schoolbook, the tensor-core schoolbook (tcgen05 int8) and the
+    NTT, operands resident in HBM, results compared word for word."""
+    import torch
+    import gpupi_b200 as g
+    torch.cuda.set_device(local)
+    ctx = g.Context()
+    L, N = args.mul_limbs, args.mul_batch
+    La, Lb = L // 2, L - L // 2
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0xB5)
+    A = torch.randint(-2 ** 31, 2 ** 31 - 1, (N * La,), dtype=torch.int32, device="cuda", generator=gen)
+    B = torch.randint(-2 ** 31, 2 ** 31 - 1, (N * Lb,), dtype=torch.int32, device="cuda", generator=gen)
+    outs, times = {}, {}
+    kernels = {"ntt": lambda C: ctx.mul_ntt(N, A.data_ptr(), La, La, B.data_ptr(), Lb, Lb, C.data_ptr(), L)}
+    if L <= 1024:
+        kernels["school"] = lambda C: g.mul_naive(N, A.data_ptr(), La, La, B.data_ptr(), Lb, Lb, C.data_ptr(), L)
+    if min(La, Lb) <= 2048 and L <= 8192:
+        kernels["tc"] = lambda C: g.mul_tc(N, A.data_ptr(), La, La, B.data_ptr(), Lb, Lb, C.data_ptr(), L)
+    for name, f in kernels.items():
+        C = torch.zeros(N * L, dtype=torch.int32, device="cuda")
+        for _ in range(args.warmup):
+            f(C)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            f(C)
+        e1.record()
+        torch.cuda.synchronize()
+        times[name] = _max_over_ranks(e0.elapsed_time(e1) / args.steps, ws)
+        outs[name] = C
+    same = all(torch.equal(outs[k], outs["ntt"]) for k in outs)
+    macs = 16.0 * La * Lb * N   # byte products of the split-integer form
+    if rank == 0:
+        print(json.dumps({"metric": f"ms for {N} products of {La} x {Lb} limbs", "value": times.get("tc"),
+                          "unit": "ms", "steps": args.steps, "warmup": args.warmup, "dtype": "u32",
+                          "ms": times, "results_equal": same, "tc_error": g.tc_error(),
+                          "tc_useful_int8_macs_per_s": macs / (times["tc"] * 1e-3) if "tc" in times else None}),
+              flush=True)
+    ctx.close()
+
+
 def run_uneven(args, ws, rank, local):
     """4096 independent products with lengths log-uniform in [8, 4096] limbs
     per operand (seeded), operands resident in HBM: one ragged call
@@ -711,10 +755,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--digits", type=int, default=1_000_000_000)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", choices=["pi", "ntt", "convert", "uneven", "intpeak"], default="pi",
+    ap.add_argument("--workload", choices=["pi", "ntt", "convert", "uneven", "intpeak", "mulsmall"], default="pi",
                     help="pi: the pi_bs_gpu pipeline (default); ntt: one large product per step; "
                          "convert: one 2^25-limb decimal conversion per step; uneven: 4096 uneven products; "
-                         "intpeak: the integer-pipe peaks")
+                         "intpeak: the integer-pipe peaks; mulsmall: one batch of equal products through "
+                         "each product kernel")
+    ap.add_argument("--mul-limbs", type=int, default=1024, help="mulsmall: L_a + L_b")
+    ap.add_argument("--mul-batch", type=int, default=16384, help="mulsmall: products per batch")
     ap.add_argument("--ntt-limbs", type=int, default=1 << 27)
     ap.add_argument("--ntt-path", choices=["fused", "spectra"], default="fused",
                     help="ntt workload: fused row pass, or forward / inverse spectra")
@@ -747,6 +794,8 @@ def main():
             run_uneven(args, ws, rank, local)
         elif args.workload == "intpeak":
             run_intpeak(args, ws, rank, local)
+        elif args.workload == "mulsmall":
+            run_mulsmall(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
         ok = True
