@@ -58,6 +58,8 @@ _SIGS = [
     ("gpupi_tc_selftest_timeout", ctypes.c_int, [ctypes.POINTER(_u32), ctypes.POINTER(_u32)]),
     ("gpupi_int_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("gpupi_fail_alloc", ctypes.c_int, [_u32, _u32]),
+    ("gpupi_tree_graph_stats", ctypes.c_int, [_p]),
+    ("gpupi_tree_graph_perturb", ctypes.c_int, []),
     ("gpupi_scratch_live_bytes", ctypes.c_uint64, []),
     ("gpupi_tune_load", ctypes.c_int, [ctypes.c_char_p]),
     ("gpupi_tune_load_text", ctypes.c_int, [ctypes.c_char_p]),
@@ -291,6 +293,18 @@ def fail_alloc(kind_mask: int, nth: int) -> None:
     """Make the nth following device allocation of a category in kind_mask
     fail once (host-side injection for error-path tests; 0 disarms)."""
     lib().gpupi_fail_alloc(kind_mask, nth)
+
+
+def tree_graph_stats() -> dict:
+    """Counts of the splitting tree's graph path (recorded schedules, captured
+    graphs, graph runs, fallbacks, sizes without a graph)."""
+    out = (ctypes.c_uint64 * 5)()
+    lib().gpupi_tree_graph_stats(ctypes.addressof(out))
+    return dict(zip(("recorded", "captured", "replayed", "fallbacks", "disabled"), map(int, out)))
+
+
+def tree_graph_perturb() -> None:
+    lib().gpupi_tree_graph_perturb()
 
 
 def scratch_live_bytes() -> int:

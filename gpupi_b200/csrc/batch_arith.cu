@@ -39,6 +39,7 @@ cudaStream_t current_stream() { return g_stream; }
 void set_current_stream(cudaStream_t s) { g_stream = s; }
 uint64_t launch_counter() { return g_launches.load(); }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(int64_t n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
 static std::atomic<uint64_t> g_h2d{0}, g_d2h{0};
 void note_h2d(uint64_t b) { g_h2d.fetch_add(b, std::memory_order_relaxed); }
@@ -270,8 +271,13 @@ BatchMPContext *batch_mp_init() {
     return ctx;
 }
 
+namespace gpupi {
+void pi_forget_context(const BatchMPContext *ctx);   // pi_engine.cu: graphs that use its tables
+}
+
 void batch_mp_destroy(BatchMPContext *ctx) {
     if (!ctx) return;
+    gpupi::pi_forget_context(ctx);
     release_context(ctx);
     delete ctx;
     gpupi::scratch_context_closed();
@@ -441,6 +447,7 @@ cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, 
     return cudaGetLastError();
 }
 const NTTPrecomputedTables &context_tables(const BatchMPContext *ctx) { return ctx->ntt_tables; }
+const void *context_workspace(const BatchMPContext *ctx) { return ctx ? ctx->workspace : nullptr; }
 void set_school_max(uint32_t v) { g_school_max = v; }
 uint32_t school_max() { return g_school_max; }
 }  // namespace gpupi

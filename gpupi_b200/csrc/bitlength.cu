@@ -194,6 +194,27 @@ static uint32_t length_max(const uint32_t *A, uint32_t *workspace, uint32_t N, u
     return *s->host;
 }
 
+// The limb length of a batch written to device memory (d_out), without a
+// host synchronisation: the same scans, the result stored where one later
+// copy reads it.  Calls on the library's stream run in order, so the shared
+// max / ticket words are never used by two at once.
+cudaError_t limb_length_to_device(const uint32_t *A, uint32_t N, uint32_t L, uint32_t stride, uint32_t *d_out) {
+    LengthState *s = length_state();
+    if (!s) return cudaErrorMemoryAllocation;
+    cudaStream_t st = current_stream();
+    if (N == 0u || L == 0u) return cudaMemsetAsync(d_out, 0, sizeof(uint32_t), st);
+    if (L <= 64u || N >= 65536u)
+        length_max_rows_kernel<false><<<grid_for(N, 256, kNumSMs * 8), 256, 0, st>>>(A, N, L, stride, s->dev,
+                                                                                   s->dev + 1, d_out);
+    else {
+        const uint64_t items = (uint64_t)N * ((L + kChunk - 1u) / kChunk);
+        length_max_chunks_kernel<false><<<grid_for(items, 1, kNumSMs * 8), 256, 0, st>>>(
+            A, N, L, stride, items, s->dev, s->dev + 1, d_out);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
 }  // namespace gpupi
 
 uint32_t batch_bitlength_max(const uint32_t *A, uint32_t *workspace, uint32_t N, uint32_t L,

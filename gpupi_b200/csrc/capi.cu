@@ -191,6 +191,22 @@ int gpupi_tc_selftest_timeout(uint32_t *seen, uint32_t *after) {
     return (int)gpupi::tc_selftest_timeout(seen, after);
 }
 
+int gpupi_tree_graph_stats(uint64_t *out5) {
+    if (!out5) return (int)cudaErrorInvalidValue;
+    const gpupi::TreeGraphStats t = gpupi::tree_graph_stats();
+    out5[0] = t.recorded;
+    out5[1] = t.captured;
+    out5[2] = t.replayed;
+    out5[3] = t.fallbacks;
+    out5[4] = t.disabled;
+    return 0;
+}
+
+int gpupi_tree_graph_perturb(void) {
+    gpupi::tree_graph_perturb();
+    return 0;
+}
+
 int gpupi_fail_alloc(uint32_t kind_mask, uint32_t nth) {
     gpupi::fail_alloc_arm(kind_mask, nth);
     return 0;

@@ -32,6 +32,7 @@ void set_current_stream(cudaStream_t s);
 // Counts kernel launches issued by this library (for launch-count claims).
 uint64_t launch_counter();
 void count_launch();
+void add_launches(int64_t n);   // kernels a CUDA graph launch runs (or un-count a capture)
 
 // Host<->device bytes moved by this library (pipeline inputs/results,
 // compact() results, base-case round trips).
@@ -49,6 +50,13 @@ void scratch_context_opened();
 void scratch_context_closed();
 void scratch_stats(uint64_t *block_bytes, uint64_t *high_water, uint64_t *spills);
 uint64_t scratch_live_bytes();
+// A caller-owned block standing in for the arena on this host thread (no
+// spills: a request that does not fit fails); see scratch.cu.
+void scratch_private_begin(void *base, size_t cap);
+bool scratch_private_end();   // false: a request did not fit
+void scratch_private_drop(void *base);
+void scratch_window_begin();
+size_t scratch_window_peak();
 
 // Host-side allocation-failure injection (tests of the error paths; no GPU
 // fault is involved): fail_alloc_arm(mask, n) makes the n-th following

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -143,8 +144,43 @@ static cudaError_t p_mul(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, Batc
                  (size_t)A.length + B.length > (size_t)BATCH_MUL_NAIVE_L_MAX,
                  [&]() { return mul_tuned(ctx, A, B, C); });
 }
+// ---------------------------------------------------------------------------
+// The splitting tree's length schedule.  Every level of the tree ends in
+// compact(): a device scan whose result the host reads back (a stream
+// synchronisation) to size the next level's rows, as in the reference.  The
+// lengths depend only on the tree size, so the first run for a size records
+// them (RECORD); later runs take them from the record and only launch the
+// scans, writing into a device array that is compared with the record once
+// the tree is done (REPLAY).  With no host synchronisation left inside it,
+// the tree can be captured into a CUDA graph (tree_run).
+// ---------------------------------------------------------------------------
+cudaError_t limb_length_to_device(const uint32_t *A, uint32_t N, uint32_t L, uint32_t stride, uint32_t *d_out);
+
+enum TreeMode { kTreeDirect = 0, kTreeRecord = 1, kTreeReplay = 2 };
+struct TreeLens {
+    TreeMode mode = kTreeDirect;
+    std::vector<uint32_t> *lens = nullptr;   // the record (written in RECORD, read in REPLAY)
+    uint32_t *d_check = nullptr;             // REPLAY: the scans' results, one word per compact
+    size_t cursor = 0;
+    bool overflow = false;                   // REPLAY met more compacts than recorded
+};
+static thread_local TreeLens t_tree;
+
 static cudaError_t p_compact(BatchMPContext *ctx, Profiler *pr, BatchMPArray &A, const char *label, uint32_t n1) {
-    return stage(pr, "compact", label, n1, A.batch_size, A.length, 0, false, [&]() { return A.compact(ctx); });
+    TreeLens &t = t_tree;
+    if (t.mode == kTreeReplay) {
+        if (t.cursor >= t.lens->size()) {
+            t.overflow = true;
+            return cudaErrorInvalidValue;
+        }
+        const cudaError_t err = limb_length_to_device(A.data, A.batch_size, A.length, A.stride, t.d_check + t.cursor);
+        A.length = (*t.lens)[t.cursor++];
+        return err;
+    }
+    const cudaError_t err =
+        stage(pr, "compact", label, n1, A.batch_size, A.length, 0, false, [&]() { return A.compact(ctx); });
+    if (err == cudaSuccess && t.mode == kTreeRecord) t.lens->push_back(A.length);
+    return err;
 }
 static cudaError_t p_shift_addsub(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, BatchMPArray B,
                                   BatchMPArray C, uint32_t shift, bool sub, uint32_t n1) {
@@ -201,6 +237,11 @@ struct Buf {
         return scratch_alloc((void **)&p, words * 4);
     }
     void swap(Buf &o) { std::swap(p, o.p); }
+    uint32_t *release() {   // give up ownership without freeing
+        uint32_t *q = p;
+        p = nullptr;
+        return q;
+    }
 };
 
 static const uint32_t kDivLo = 830297u;       // pi_bs_gpu.cu:147
@@ -449,6 +490,263 @@ static cudaError_t binary_split(BatchMPContext *ctx, Profiler *pr, uint32_t N, B
     }
     qbuf.swap(qb);
     rbuf.swap(rb);
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// The splitting tree as a CUDA graph.
+//
+// Per (context, tree size, form): the first run records the length schedule
+// (and the tree's peak of scratch bytes); the second captures the tree with
+// the recorded lengths (no host synchronisation inside) into a graph, its
+// temporaries carved from a private device block so that the graph's
+// addresses stay valid; every later run launches that graph on the
+// library's tree stream (ordered after and before the caller's stream by
+// events) and checks the lengths the device computed against the schedule
+// with one copy.  A disagreement (never expected: the computation is
+// deterministic) runs the tree directly and records again, so the result is
+// always the exact one.  Q and R then live in the private block until the
+// next run of the same graph.  Not used while the stage profiler or the
+// kernel timers are on (both time individual launches), when the block
+// would not leave 8 GB of the device free, or with GPUPI_TREE_GRAPH=0.
+// ---------------------------------------------------------------------------
+namespace {
+struct TreeGraph {
+    const BatchMPContext *ctx = nullptr;
+    int dev = -1;
+    uint32_t N = 0;
+    bool tuned = false;
+    int state = 0;   // 0 nothing, 1 schedule recorded, 2 graph captured, 3 graph not possible
+    std::vector<uint32_t> lens;
+    size_t peak = 0;
+    void *pool = nullptr;
+    size_t pool_cap = 0;
+    uint32_t *d_check = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t *q = nullptr, *r = nullptr;
+    uint32_t lq = 0, lr = 0;
+    int64_t launches = 0;
+    const void *ws = nullptr;
+    size_t ws_size = 0;
+};
+std::mutex g_tree_mu;
+std::vector<TreeGraph> g_trees;
+TreeGraphStats g_tree_stats{};
+
+void tree_release(TreeGraph &g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.pool) {
+        scratch_private_drop(g.pool);
+        cudaFree(g.pool);
+    }
+    if (g.d_check) cudaFree(g.d_check);
+    g.exec = nullptr;
+    g.pool = nullptr;
+    g.d_check = nullptr;
+    g.q = g.r = nullptr;
+}
+
+cudaStream_t tree_stream(int dev) {
+    static cudaStream_t s[64] = {};
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!s[dev] && cudaStreamCreateWithFlags(&s[dev], cudaStreamNonBlocking) != cudaSuccess) s[dev] = nullptr;
+    return s[dev];
+}
+
+bool tree_graphs_enabled() {
+    const char *e = getenv("GPUPI_TREE_GRAPH");
+    return !(e && e[0] == '0');
+}
+}  // namespace
+
+TreeGraphStats tree_graph_stats() {
+    std::lock_guard<std::mutex> l(g_tree_mu);
+    return g_tree_stats;
+}
+
+void tree_graph_perturb() {
+    std::lock_guard<std::mutex> l(g_tree_mu);
+    for (TreeGraph &g : g_trees)
+        if (!g.lens.empty() && g.lens[0] > 1u) g.lens[0] -= 1u;
+}
+
+void pi_forget_context(const BatchMPContext *ctx) {
+    std::lock_guard<std::mutex> l(g_tree_mu);
+    for (auto it = g_trees.begin(); it != g_trees.end();) {
+        if (it->ctx == ctx) {
+            int cur = 0;
+            cudaGetDevice(&cur);
+            if (it->dev != cur) cudaSetDevice(it->dev);
+            cudaDeviceSynchronize();
+            tree_release(*it);
+            if (it->dev != cur) cudaSetDevice(cur);
+            it = g_trees.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+// Captures the tree into g (state 1 -> 2).  Returns cudaSuccess with
+// *usable false when a graph is not possible here (a capture-specific
+// failure: the tree then runs directly), or the error of the tree itself.
+static cudaError_t tree_capture(BatchMPContext *ctx, TreeGraph &g, bool *usable) {
+    *usable = false;
+    const size_t cap = g.peak + g.peak / 4 + ((size_t)64 << 20);
+    // the block comes on top of the stream's arena: only with room to spare
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || cap + ((size_t)8 << 30) > free_b) {
+        cudaGetLastError();
+        return cudaSuccess;
+    }
+    if (cudaMalloc(&g.pool, cap) != cudaSuccess ||
+        cudaMalloc((void **)&g.d_check, std::max<size_t>(1, g.lens.size()) * 4) != cudaSuccess) {
+        cudaGetLastError();
+        tree_release(g);
+        return cudaSuccess;
+    }
+    g.pool_cap = cap;
+    cudaStream_t st = current_stream(), ts = tree_stream(g.dev);
+    if (!ts) {
+        tree_release(g);
+        return cudaSuccess;
+    }
+    const uint64_t l0 = launch_counter();
+    t_tree = TreeLens{};
+    t_tree.mode = kTreeReplay;
+    t_tree.lens = &g.lens;
+    t_tree.d_check = g.d_check;
+    set_current_stream(ts);
+    scratch_private_begin(g.pool, cap);
+    cudaGraph_t graph = nullptr;
+    Buf q, r;
+    BatchMPArray Q, R;
+    cudaError_t err = cudaStreamBeginCapture(ts, cudaStreamCaptureModeThreadLocal);
+    const bool began = err == cudaSuccess;
+    if (began) err = binary_split(ctx, nullptr, g.N, q, Q, r, R, g.tuned);
+    const cudaError_t cerr = began ? cudaStreamEndCapture(ts, &graph) : err;
+    const bool fits = scratch_private_end();
+    set_current_stream(st);
+    const bool complete = !t_tree.overflow && t_tree.cursor == g.lens.size();
+    t_tree = TreeLens{};
+    const int64_t recorded = (int64_t)(launch_counter() - l0);
+    add_launches(-recorded);   // captured, not run: counted at each launch of the graph
+    g.launches = 0;
+    if (began && err == cudaSuccess && cerr == cudaSuccess && fits && complete && graph &&
+        cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        g.q = q.release();
+        g.r = r.release();
+        g.lq = Q.length;
+        g.lr = R.length;
+        g.ws = context_workspace(ctx);
+        g.ws_size = batch_mp_workspace_size(ctx);
+        g.launches = recorded;
+        g.state = 2;
+        *usable = true;
+        return cudaSuccess;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    q.reset();
+    r.reset();
+    tree_release(g);
+    // an error of the tree itself (not of capturing it) is the caller's
+    if (began && err != cudaSuccess && fits && cerr == cudaSuccess) return err;
+    return cudaSuccess;
+}
+
+static cudaError_t tree_run(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &qbuf, BatchMPArray &Q, Buf &rbuf,
+                            BatchMPArray &R, bool tuned) {
+    if (!tree_graphs_enabled() || (pr && pr->on) || kernel_timer_enabled())
+        return binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::unique_lock<std::mutex> lock(g_tree_mu);
+    TreeGraph *g = nullptr;
+    for (TreeGraph &x : g_trees)
+        if (x.ctx == ctx && x.dev == dev && x.N == N && x.tuned == tuned) g = &x;
+    if (!g) {
+        g_trees.push_back(TreeGraph{});
+        g = &g_trees.back();
+        g->ctx = ctx;
+        g->dev = dev;
+        g->N = N;
+        g->tuned = tuned;
+    }
+    if (g->state == 3) {
+        lock.unlock();
+        return binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
+    }
+    if (g->state == 2 && (g->ws != context_workspace(ctx) || g->ws_size != batch_mp_workspace_size(ctx))) {
+        tree_release(*g);   // the graph's products used another workspace
+        g->state = 1;
+    }
+    if (g->state == 0) {
+        std::vector<uint32_t> lens;
+        t_tree = TreeLens{};
+        t_tree.mode = kTreeRecord;
+        t_tree.lens = &lens;
+        scratch_window_begin();
+        const cudaError_t err = binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
+        const size_t peak = scratch_window_peak();
+        t_tree = TreeLens{};
+        if (err != cudaSuccess) return err;
+        g->lens.swap(lens);
+        g->peak = peak;
+        g->state = 1;
+        ++g_tree_stats.recorded;
+        return cudaSuccess;
+    }
+    if (g->state == 1) {
+        bool usable = false;
+        const cudaError_t err = tree_capture(ctx, *g, &usable);
+        if (err != cudaSuccess) return err;
+        if (!usable) {
+            g->state = 3;
+            ++g_tree_stats.disabled;
+            lock.unlock();
+            return binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
+        }
+        ++g_tree_stats.captured;
+    }
+    // launch the graph after the caller's stream's work, and the caller's
+    // stream after it
+    cudaStream_t st = current_stream(), ts = tree_stream(dev);
+    static cudaEvent_t evs[64][2] = {};
+    cudaEvent_t *ev = evs[dev & 63];
+    if (!ev[0]) {
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    }
+    cudaError_t err = cudaEventRecord(ev[0], st);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(ts, ev[0], 0);
+    if (err == cudaSuccess) err = cudaGraphLaunch(g->exec, ts);
+    if (err == cudaSuccess) err = cudaEventRecord(ev[1], ts);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(st, ev[1], 0);
+    if (err != cudaSuccess) return err;
+    add_launches(g->launches);
+    // the lengths the device found, against the schedule the graph used
+    std::vector<uint32_t> seen(g->lens.size());
+    if (!seen.empty()) {
+        err = cudaMemcpyAsync(seen.data(), g->d_check, seen.size() * 4, cudaMemcpyDeviceToHost, st);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+        if (err != cudaSuccess) return err;
+        note_d2h(seen.size() * 4);
+    }
+    if (seen != g->lens) {
+        ++g_tree_stats.fallbacks;
+        tree_release(*g);
+        g->lens.clear();
+        g->state = 0;
+        lock.unlock();
+        return binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
+    }
+    ++g_tree_stats.replayed;
+    qbuf.reset();
+    rbuf.reset();
+    Q = BatchMPArray{g->q, g->lq, 1, g->lq};
+    R = BatchMPArray{g->r, g->lr, 1, g->lr};
     return cudaSuccess;
 }
 
@@ -758,7 +1056,7 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     if (ckpt && ckpt_load(ckpt, N, qbs, Qbs, rbs, Rbs)) {
         *ckpt_state = 1;
     } else {
-        TRY(binary_split(ctx, pr, N, qbs, Qbs, rbs, Rbs, tuned));
+        TRY(tree_run(ctx, pr, N, qbs, Qbs, rbs, Rbs, tuned));
         if (ckpt) {
             // a file that cannot be written (unwritable directory, full
             // disk) does not fail the computation: state 3 reports it

@@ -64,6 +64,18 @@ cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, 
 // batch_mp_mul with this library's schoolbook/NTT crossover (school_max()).
 cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 const NTTPrecomputedTables &context_tables(const BatchMPContext *ctx);
+const void *context_workspace(const BatchMPContext *ctx);
+void pi_forget_context(const BatchMPContext *ctx);
+// The splitting tree as a CUDA graph: counts of runs that recorded the
+// length schedule, captured the graph, replayed it, fell back after the
+// device's lengths disagreed with the schedule, and of sizes where no graph
+// was possible; perturb alters every recorded schedule (tests of the
+// fallback).
+struct TreeGraphStats {
+    uint64_t recorded, captured, replayed, fallbacks, disabled;
+};
+TreeGraphStats tree_graph_stats();
+void tree_graph_perturb();
 void set_school_max(uint32_t v);
 uint32_t school_max();
 

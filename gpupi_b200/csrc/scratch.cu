@@ -47,8 +47,14 @@ struct Arena {
     std::unordered_map<void *, size_t> live;        // arena blocks: ptr -> size
     std::unordered_map<void *, size_t> spilled;     // cudaMallocAsync blocks: ptr -> size
     size_t live_bytes = 0, high = 0;
+    size_t win_base = 0, win_peak = 0;   // live bytes at a window's start, peak above it
     uint64_t spills = 0;   // requests ever served outside the block
     bool grow = false;
+
+    void note_peak() {
+        high = std::max(high, live_bytes);
+        if (live_bytes > win_base) win_peak = std::max(win_peak, live_bytes - win_base);
+    }
 
     void reset_block(char *p, size_t bytes) {
         base = p;
@@ -63,7 +69,7 @@ struct Arena {
             void *p = base + off;
             live.emplace(p, need);
             live_bytes += need;
-            high = std::max(high, live_bytes);
+            note_peak();
             *out = p;
             return cudaSuccess;
         }
@@ -73,7 +79,7 @@ struct Arena {
         spilled.emplace(p, need);
         ++spills;
         live_bytes += need;
-        high = std::max(high, live_bytes);
+        note_peak();
         grow = true;
         *out = p;
         return cudaSuccess;
@@ -130,11 +136,27 @@ struct Arena {
     }
 };
 
+// A caller-owned device block carved like an arena but never spilling: the
+// splitting tree's temporaries while the tree is captured into a CUDA graph
+// (pi_engine.cu), so that every replay of the graph finds them at the same
+// addresses.  Selected per host thread; its ranges are recognised by
+// address when freed later.
+struct Private {
+    char *base = nullptr;
+    size_t cap = 0;
+    RangeMap free;
+    std::unordered_map<void *, size_t> live;
+    bool exhausted = false;   // a request did not fit
+};
+
 struct Registry {
     std::mutex mu;
     std::map<std::pair<int, cudaStream_t>, Arena> arenas;
+    std::map<char *, Private> privates;   // by base
     int contexts = 0;
 };
+
+thread_local char *t_private = nullptr;   // base of this thread's active private block
 Registry &registry() {
     static Registry r;
     return r;
@@ -164,6 +186,20 @@ bool fail_alloc_now(AllocKind kind) {
 cudaError_t scratch_alloc(void **p, size_t bytes) {
     if (!p) return cudaErrorInvalidValue;
     if (fail_alloc_now(kAllocScratch)) return cudaErrorMemoryAllocation;
+    if (t_private) {
+        Registry &r = registry();
+        std::lock_guard<std::mutex> g(r.mu);
+        Private &pv = r.privates[t_private];
+        const size_t need = round_up(bytes ? bytes : 1, kAlign);
+        size_t off = 0;
+        if (!pv.free.take(need, &off)) {
+            pv.exhausted = true;
+            return cudaErrorMemoryAllocation;
+        }
+        *p = pv.base + off;
+        pv.live.emplace(*p, need);
+        return cudaSuccess;
+    }
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
@@ -179,8 +215,74 @@ void scratch_free(void *p) {
     if (!p) return;
     Registry &r = registry();
     std::lock_guard<std::mutex> g(r.mu);
+    if (!r.privates.empty()) {
+        auto it = r.privates.upper_bound((char *)p);
+        if (it != r.privates.begin()) {
+            --it;
+            Private &pv = it->second;
+            if ((char *)p < pv.base + pv.cap) {
+                auto a = pv.live.find(p);
+                if (a != pv.live.end()) {
+                    pv.free.give((size_t)((char *)p - pv.base), a->second);
+                    pv.live.erase(a);
+                }
+                return;
+            }
+        }
+    }
     for (auto &kv : r.arenas)
         if (kv.second.release(p)) return;
+}
+
+// Start carving the calling thread's scratch requests from [base, base + cap)
+// (freshly: every range free); scratch_private_end() returns to the stream
+// arenas and reports whether every request fitted.
+void scratch_private_begin(void *base, size_t cap) {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    Private &pv = r.privates[(char *)base];
+    pv.base = (char *)base;
+    pv.cap = cap;
+    pv.free.reset(cap);
+    pv.live.clear();
+    pv.exhausted = false;
+    t_private = (char *)base;
+}
+
+bool scratch_private_end() {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    const bool ok = t_private ? !r.privates[t_private].exhausted : true;
+    t_private = nullptr;
+    return ok;
+}
+
+// Forget a private block (its memory is the caller's to free).
+void scratch_private_drop(void *base) {
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    r.privates.erase((char *)base);
+}
+
+// Peak of live scratch bytes on the current stream's arena above the level
+// at scratch_window_begin().
+void scratch_window_begin() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    Arena &a = r.arenas[{dev, current_stream()}];
+    a.stream = current_stream();
+    a.win_base = a.live_bytes;
+    a.win_peak = 0;
+}
+
+size_t scratch_window_peak() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    Registry &r = registry();
+    std::lock_guard<std::mutex> g(r.mu);
+    return r.arenas[{dev, current_stream()}].win_peak;
 }
 
 void scratch_reserve(size_t bytes) {

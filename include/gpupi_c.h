@@ -99,6 +99,20 @@ int gpupi_tc_error(void);
  * context stay usable).  No GPU fault is involved. */
 int gpupi_tc_selftest_timeout(uint32_t *seen, uint32_t *after);
 
+/* The splitting tree as a CUDA graph (no counterpart in the reference,
+ * whose tree synchronises with the host at every compact()): for each
+ * context, tree size and form, the first gpupi_pi_compute records the
+ * length schedule, the second captures the tree into a graph, later ones
+ * launch it and check the device's lengths against the schedule with one
+ * copy (a mismatch runs the tree directly; results are always the exact
+ * ones).  out5 = {schedules recorded, graphs captured, graph runs,
+ * fallbacks after a mismatch, sizes where a graph was not possible}.
+ * gpupi_tree_graph_perturb alters every recorded schedule so that the next
+ * graph run exercises the fallback (testing).  GPUPI_TREE_GRAPH=0 in the
+ * environment runs the tree directly. */
+int gpupi_tree_graph_stats(uint64_t *out5);
+int gpupi_tree_graph_perturb(void);
+
 /* Error-path testing (no counterpart in the reference, whose allocations
  * are partly unchecked, pi_bs_gpu.cu:1199-1203): the nth following device
  * allocation whose category is in kind_mask fails once with
