@@ -794,7 +794,36 @@ struct CrtArgs {
     uint32_t Lc;
     uint32_t tiles;
     uint32_t *flags;
+    uint32_t ncoef;      // coefficients of the product (L_a + L_b - 1)
+    // optional addend: C = product + (D << dshift), D rows at D + row * sD,
+    // Ld limbs; C's L_c limbs must hold the sum
+    const uint32_t *D;
+    uint64_t sD;
+    uint32_t Ld;
+    uint32_t dshift;
 };
+
+// Adds limbs base .. base + kCrtV - 1 of (D << dshift) to the chunk sum S
+// (carries run into S's three top words, which stay far from overflowing).
+__device__ __forceinline__ void crt_add_shifted(const CrtArgs &a, const uint32_t *Dr, int64_t base,
+                                                uint32_t (&S)[kCrtV + 3]) {
+    const int64_t sw = a.dshift >> 5;
+    const uint32_t sb = a.dshift & 31u;
+    uint64_t cy = 0;
+#pragma unroll
+    for (int v = 0; v < kCrtV + 3; ++v) {
+        uint32_t d = 0u;
+        if (v < kCrtV) {
+            const int64_t i = base + v - sw;   // source limb of the low part
+            const uint32_t lo = (i >= 0 && i < (int64_t)a.Ld) ? Dr[i] : 0u;
+            const uint32_t hi = (sb && i - 1 >= 0 && i - 1 < (int64_t)a.Ld) ? Dr[i - 1] : 0u;
+            d = sb ? ((lo << sb) | (hi >> (32u - sb))) : lo;
+        }
+        const uint64_t t = (uint64_t)S[v] + d + cy;
+        S[v] = (uint32_t)t;
+        cy = t >> 32;
+    }
+}
 
 // Coefficient n of a row lives in block b = n / K at F0[(b * 3 + q) * K + n mod K];
 // there are ncoef = L_c - 1 <= M K of them (the top limb only receives carries).
@@ -839,7 +868,9 @@ __global__ void __launch_bounds__(kThreads) k_crt(CrtArgs a) {
     const int64_t base = (int64_t)t * kCrtSpan + threadIdx.x * kCrtV;
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     uint32_t S[kCrtV + 3];
-    crt_chunk(F0, a.log_k, a.Lc - 1u, base, S);
+    const uint32_t *Dr = a.D ? a.D + row * a.sD : nullptr;
+    crt_chunk(F0, a.log_k, a.ncoef, base, S);
+    if (Dr) crt_add_shifted(a, Dr, base, S);
     // words of the previous chunk's sum that land in this chunk: from the
     // previous lane, from the previous warp's last lane, and for the tile's
     // first thread from the last chunk of the previous tile (recomputed)
@@ -854,7 +885,8 @@ __global__ void __launch_bounds__(kThreads) k_crt(CrtArgs a) {
     }
     if (threadIdx.x == 0) {
         uint32_t Sp[kCrtV + 3];
-        crt_chunk(F0, a.log_k, a.Lc - 1u, base - kCrtV, Sp);
+        crt_chunk(F0, a.log_k, a.ncoef, base - kCrtV, Sp);
+        if (Dr) crt_add_shifted(a, Dr, base - kCrtV, Sp);
         H[0] = Sp[kCrtV];
         H[1] = Sp[kCrtV + 1];
         H[2] = Sp[kCrtV + 2];
@@ -1202,7 +1234,7 @@ static void mul(const NttParams &P, const uint32_t *A, const uint32_t *B, uint32
             launch_combine(M, P, c, N, st);
         }
     }
-    CrtArgs c{FA, log_k, M, C, sC, Lc, (uint32_t)tiles, flags};
+    CrtArgs c{FA, log_k, M, C, sC, Lc, (uint32_t)tiles, flags, Lc - 1u, nullptr, 0, 0, 0};
     KernelTimed kt("ntt_crt_carry", 12.0 * (double)Lc * N + 4.0 * (double)Lc * N);
     k_crt<<<(unsigned)(N * tiles), kThreads, 0, st>>>(c);
     count_launch();
@@ -1261,7 +1293,7 @@ static void spectrum_forward(const NttParams &P, Shape s, uint32_t N, const uint
 
 static void spectrum_inverse(const NttParams &P, Shape s, uint32_t N, int terms, const uint32_t *const *X,
                              const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC, uint32_t Lc,
-                             uint32_t *flags, cudaStream_t st, bool rows) {
+                             uint32_t *flags, cudaStream_t st, bool rows, const SpectrumAddend *add) {
     const int log_k = s.log_k, M = s.M;
     const uint64_t K = 1ull << log_k;
     const uint64_t VR = (uint64_t)N * M;
@@ -1301,8 +1333,16 @@ static void spectrum_inverse(const NttParams &P, Shape s, uint32_t N, int terms,
         launch_combine(M, P, c, N, st);
     }
     const uint64_t tiles = ((uint64_t)Lc + kCrtSpan - 1) / kCrtSpan;
-    CrtArgs c{Fout, log_k, M, C, sC, Lc, (uint32_t)tiles, flags};
-    KernelTimed kt("ntt_crt_carry", 12.0 * (double)Lc * N + 4.0 * (double)Lc * N);
+    CrtArgs c{Fout, log_k, M, C, sC, Lc, (uint32_t)tiles, flags, Lc - 1u, nullptr, 0, 0, 0};
+    if (add) {
+        c.ncoef = add->ncoef;
+        c.D = add->D;
+        c.sD = add->sD;
+        c.Ld = add->Ld;
+        c.dshift = add->shift;
+    }
+    KernelTimed kt("ntt_crt_carry", 12.0 * (double)c.ncoef * N + 4.0 * (double)Lc * N +
+                                        (add ? 4.0 * (double)add->Ld * N : 0.0));
     k_crt<<<(unsigned)(N * tiles), kThreads, 0, st>>>(c);
     count_launch();
     if (tiles > 1) launch_carry_fixup(false, C, sC, N, Lc, (uint32_t)tiles, kCrtSpan, flags, st);
@@ -1431,10 +1471,10 @@ void spectrum_forward(const NTTPrecomputedTables &tables, SpectrumShape s, uint3
 
 void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, int terms,
                       const uint32_t *const *X, const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC,
-                      uint32_t Lc, uint32_t *flags, bool rows) {
+                      uint32_t Lc, uint32_t *flags, bool rows, const SpectrumAddend *add) {
     const ntt::NttParams P = ntt::make_params(tables);
     ntt::spectrum_inverse(P, ntt::Shape{s.log_k, s.M}, N, terms, X, Y, Fout, C, sC, Lc, flags, current_stream(),
-                          rows);
+                          rows, add);
 }
 
 void spectrum_level_rows(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, uint32_t *Fpe,

@@ -330,7 +330,11 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
     const BatchMPArray Q_even{Q.data, lq, half, Q.stride * 2}, Q_odd{Q.data + Q.stride, lq, half, Q.stride * 2};
     const BatchMPArray R_even{R.data, lr, half, R.stride * 2}, R_odd{R.data + R.stride, lr, half, R.stride * 2};
     Buf fpe, fpo, fqe, fqo, fre, fro, flags, r1b, r2b;
-    TRY(flags.alloc(spectrum_flag_words(half, std::max(std::max(lr + lq, 2u * lq), std::max(lr + lp, 2u * lp)))));
+    const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
+    const uint32_t r1_shifted = lr + lq + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
+    const uint32_t rlen = std::max(r1_shifted, lr + lp) + (subtract ? 0u : 1u);
+    TRY(flags.alloc(spectrum_flag_words(
+        half, std::max(std::max(std::max(lr + lq, 2u * lq), std::max(lr + lp, 2u * lp)), rlen))));
     // column passes of the six operands, two per launch: P_e and P_o share
     // the pb rows they both have (P_e's last row follows alone when P has an
     // odd row count; P_o's row there is left unset and its product unused)
@@ -376,15 +380,24 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
     TRY(p_compact(ctx, pr, Qn, "Q", n1));
     const BatchMPArray R1{nullptr, lr + lq, half, lr + lq}, R2{nullptr, lr + lp, half, lr + lp};
     TRY(r1b.alloc((size_t)half * R1.stride));
-    TRY(r2b.alloc((size_t)half * R2.stride));
     TRY(finish("R*Q", half, fre, r1b.p, R1.length, lr, lq));
-    TRY(finish("P*R", half, fro, r2b.p, R2.length, lp, lr));
-    const uint32_t shift = 15u * ((n / n1) + ((n / n1) >> 4));
-    const uint32_t r1_shifted = R1.length + (shift >> 5) + ((shift & 31u) != 0u ? 1u : 0u);
-    const uint32_t rlen = std::max(r1_shifted, R2.length) + (subtract ? 0u : 1u);
     Rn = BatchMPArray{nullptr, rlen, half, rlen};
     TRY(rn.alloc((size_t)half * rlen));
     Rn.data = rn.p;
+    if (!subtract) {
+        // R' = (R1 << s) + R2 straight out of R2's CRT and carry pass: R1's
+        // shifted limbs join the carry chain, R2 is never stored and no
+        // separate addition pass runs (same integers as the plain level)
+        const SpectrumAddend add{r1b.p, R1.stride, R1.length, shift, lr + lp - 1u};
+        TRY(stage(pr, "mul", "P*R+(R*Q<<15n)", n1, half, lp, lr, true, [&]() {
+            spectrum_inverse(tab, S, half, 1, nullptr, nullptr, fro.p, Rn.data, rlen, rlen, flags.p, false, &add);
+            fro.reset();
+            return cudaGetLastError();
+        }));
+        return p_compact(ctx, pr, Rn, "R", n1);
+    }
+    TRY(r2b.alloc((size_t)half * R2.stride));
+    TRY(finish("P*R", half, fro, r2b.p, R2.length, lp, lr));
     TRY(p_shift_addsub(ctx, pr, BatchMPArray{r1b.p, R1.length, half, R1.stride},
                        BatchMPArray{r2b.p, R2.length, half, R2.stride}, Rn, shift, subtract, n1));
     return p_compact(ctx, pr, Rn, "R", n1);

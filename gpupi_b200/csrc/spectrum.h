@@ -36,14 +36,26 @@ bool spectrum_sum_fits(const uint32_t *La, const uint32_t *Lb, int terms);
 void spectrum_forward(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, const uint32_t *X,
                       uint64_t sX, uint32_t Lx, uint32_t *FX, const uint32_t *Y, uint64_t sY, uint32_t Ly,
                       uint32_t *FY, bool rows = true);
-// C rows (stride sC, Lc limbs) = sum over terms (<= 2) of X_t Y_t.  Fout
-// receives the intermediate residues and may be one of the X_t / Y_t;
-// flags: spectrum_flag_words(N, Lc) words.
+// An addend folded into the CRT and carry pass: C = product + (D << shift)
+// (D rows at D + i * sD, Ld limbs); the product has ncoef coefficients and
+// C's Lc limbs must hold the sum.  It replaces a separate shifted-addition
+// pass (and the product's own buffer).
+struct SpectrumAddend {
+    const uint32_t *D;
+    uint64_t sD;
+    uint32_t Ld;
+    uint32_t shift;
+    uint32_t ncoef;
+};
+
+// C rows (stride sC, Lc limbs) = sum over terms (<= 2) of X_t Y_t (plus the
+// addend when add is not null).  Fout receives the intermediate residues and
+// may be one of the X_t / Y_t; flags: spectrum_flag_words(N, Lc) words.
 // rows = false: Fout already holds the product after its inverse row pass
 // (spectrum_level_rows); X and Y are not read.
 void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, int terms,
                       const uint32_t *const *X, const uint32_t *const *Y, uint32_t *Fout, uint32_t *C, uint64_t sC,
-                      uint32_t Lc, uint32_t *flags, bool rows = true);
+                      uint32_t Lc, uint32_t *flags, bool rows = true, const SpectrumAddend *add = nullptr);
 
 // One merge level's row products from six column-transformed operands
 // (spectrum_forward with rows = false): P' = P_e P_o into Fpo, R2 = P_e R_o
