@@ -626,7 +626,7 @@ struct RowsLevelArgs {
 
 template <int Q>
 __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLevelArgs &a, uint64_t b,
-                                                uint32_t *Sm, uint2 *tw, uint32_t *held) {
+                                                uint32_t *Sm, uint2 *tw) {
     constexpr int C = 1 << kSplitLogC;
     constexpr int T = C / 16;
     using First = typename ExecStage<kSplitLogC, 0, false, 0>::S;
@@ -660,8 +660,11 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
         __syncthreads();
     };
     // kept operand F_keep; products F_keep F0 -> F0, F_keep F1 -> F1.  The
-    // first product waits in the thread's own slots of `held` (word j of
-    // thread t at j * T + t: conflict-free) while the second is formed.
+    // first product waits in F0's own segment (word j of thread t at
+    // j * T + t, coalesced; every thread has loaded F0 before the stages'
+    // barriers, and reads back only its own words) while the second is
+    // formed: the segment is rewritten by the product's inverse anyway, and
+    // keeping it out of shared memory leaves room for a fourth CTA per SM.
     auto half = [&](const uint32_t *F_keep, uint32_t *F0, uint32_t *F1) {
         uint32_t k[16], x[16];
         table(levf);
@@ -670,6 +673,7 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
         __syncthreads();
         load(F0, x);
         run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
+        uint32_t *held = F0 + off;
 #pragma unroll
         for (int j = 0; j < 16; ++j) held[j * T + t] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
         __syncthreads();
@@ -699,23 +703,22 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
     half(a.Fqo, a.Fqe, a.Fre);
 }
 
-// the padded tile, the twiddle levels, one held product
-constexpr size_t rows_level_smem_bytes() { return rows_smem_bytes<kSplitLogC>() + (size_t)(1 << kSplitLogC) * 4u; }
+// the padded tile and the twiddle levels
+constexpr size_t rows_level_smem_bytes() { return rows_smem_bytes<kSplitLogC>(); }
 
-__global__ void __launch_bounds__((1 << kSplitLogC) / 16, 3) k_rows_level(NttParams P, RowsLevelArgs a) {
+__global__ void __launch_bounds__((1 << kSplitLogC) / 16, 4) k_rows_level(NttParams P, RowsLevelArgs a) {
     extern __shared__ uint4 rows_smem[];
     constexpr int C = 1 << kSplitLogC;
     uint32_t *Sm = reinterpret_cast<uint32_t *>(rows_smem);
     uint2 *tw = reinterpret_cast<uint2 *>(Sm + C + C / 32);
-    uint32_t *held = reinterpret_cast<uint32_t *>(tw + (C - 1));
     uint64_t b;
     const int q = grid_prime(b);
     if (q == 0)
-        rows_level_body<0>(P, a, b, Sm, tw, held);
+        rows_level_body<0>(P, a, b, Sm, tw);
     else if (q == 1)
-        rows_level_body<1>(P, a, b, Sm, tw, held);
+        rows_level_body<1>(P, a, b, Sm, tw);
     else
-        rows_level_body<2>(P, a, b, Sm, tw, held);
+        rows_level_body<2>(P, a, b, Sm, tw);
 }
 
 // Coset recombination.  Row r holds z_i[j] = C_i[j] g^(ij) for cosets i < M;
