@@ -618,7 +618,8 @@ __global__ void __launch_bounds__((1 << kSplitLogC) / 16, 4) k_rows_inv(NttParam
 // CTA forms P' = P_e P_o, R2 = P_e R_o, Q' = Q_e Q_o, R1 = R_e Q_o (each
 // x K^-1) and runs their inverse row stages, writing them over P_o, R_o, Q_e
 // and R_e: six forward and four inverse row transforms, the kept operand
-// (P_e, then Q_o) and one product in registers, no spectrum stored.
+// (P_e, then Q_o) and one product in registers, no spectrum stored.  With
+// Fpo null (the tree's root) P' is not formed: five and three.
 struct RowsLevelArgs {
     uint32_t *Fpe, *Fpo, *Fro, *Fqo, *Fqe, *Fre;
     int log_k;
@@ -665,17 +666,20 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
     // barriers, and reads back only its own words) while the second is
     // formed: the segment is rewritten by the product's inverse anyway, and
     // keeping it out of shared memory leaves room for a fourth CTA per SM.
+    // F0 null (uniform over the grid): the product F_keep F1 alone.
     auto half = [&](const uint32_t *F_keep, uint32_t *F0, uint32_t *F1) {
         uint32_t k[16], x[16];
         table(levf);
         load(F_keep, k);
         run_stages<kSplitLogC, 0, false, Q, 0>(k, Sm, t, tw);
-        __syncthreads();
-        load(F0, x);
-        run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
-        uint32_t *held = F0 + off;
+        uint32_t *held = F0 ? F0 + off : nullptr;
+        if (held) {
+            __syncthreads();
+            load(F0, x);
+            run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) held[j * T + t] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
+            for (int j = 0; j < 16; ++j) held[j * T + t] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
+        }
         __syncthreads();
         load(F1, x);
         run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
@@ -684,11 +688,13 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
         table(levi);
         run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
         store(F1, x);
-        __syncthreads();
+        if (held) {
+            __syncthreads();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = held[j * T + t];
-        run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
-        store(F0, x);
+            for (int j = 0; j < 16; ++j) x[j] = held[j * T + t];
+            run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
+            store(F0, x);
+        }
     };
     // The six operand segments (16 KiB each, contiguous, 16-byte aligned) go
     // to L2 by bulk prefetch (the copy engine, no registers or shared memory)
@@ -697,7 +703,9 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
     if (t < 6u) {
         const uint32_t *F = t == 0u ? a.Fpe : t == 1u ? a.Fpo : t == 2u ? a.Fro : t == 3u ? a.Fqo
                                                                       : t == 4u ? a.Fqe : a.Fre;
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F + off), "r"((uint32_t)C * 4u) : "memory");
+        if (F)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F + off), "r"((uint32_t)C * 4u)
+                         : "memory");
     }
     half(a.Fpe, a.Fpo, a.Fro);
     half(a.Fqo, a.Fqe, a.Fre);
@@ -1488,7 +1496,8 @@ void spectrum_level_rows(const NTTPrecomputedTables &tables, SpectrumShape s, ui
     const uint64_t VR = (uint64_t)N * s.M;
     const unsigned blocks = (unsigned)(VR * ntt::kPrimes * ((1ull << s.log_k) >> ntt::kSplitLogC));
     ntt::RowsLevelArgs a{Fpe, Fpo, Fro, Fqo, Fqe, Fre, s.log_k};
-    KernelTimed kt("ntt_rows_level", 40.0 * (double)(1ull << s.log_k) * (double)VR * ntt::kPrimes);
+    // six residues read and four written per point, or five and three
+    KernelTimed kt("ntt_rows_level", (Fpo ? 40.0 : 32.0) * (double)(1ull << s.log_k) * (double)VR * ntt::kPrimes);
     ntt::k_rows_level<<<blocks, (1 << ntt::kSplitLogC) / 16, ntt::rows_level_smem_bytes(), st>>>(P, a);
     count_launch();
 }

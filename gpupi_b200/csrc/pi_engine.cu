@@ -302,10 +302,12 @@ static cudaError_t plain_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
 // six forward transforms instead of eight (four inverse either way): the
 // six operands' column passes, then one row kernel for the four products
 // (spectrum_level_rows), then each product's inverse column passes and
-// CRT; R' = (R1 << s) +- R2 as in the plain level.  Used when all four products
-// have the same transform shape (summing R' in the transform domain would
-// need room for R1 << s, about 6 % longer than R1, which sits just below a
-// power of two at every level and would double the transforms).  The
+// CRT; R' = (R1 << s) +- R2 as in the plain level.  All products run at the
+// largest one's transform shape; used when that costs less than the plain
+// level (summing R' in the transform domain would need room for R1 << s,
+// about 6 % longer than R1, which sits just below a power of two at every
+// level and would double the transforms).  At the root P' is not formed
+// (as in the plain level): five forward and three inverse transforms.  The
 // integers are those of the plain level.  *done = false (nothing issued)
 // when the level does not qualify.
 // ---------------------------------------------------------------------------
@@ -315,14 +317,27 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
                                BatchMPArray &Rn, bool *done) {
     *done = false;
     const uint32_t lp = P.length, lq = Q.length, lr = R.length;
-    const uint32_t pb = half - ignore;   // rows of P'
-    const SpectrumShape S = spectrum_shape((uint64_t)lr + lq - 1u);
-    if (S.M == 0 || pb == 0u) return cudaSuccess;
-    const uint64_t needs[3] = {2ull * lq - 1u, (uint64_t)lp + lr - 1u, 2ull * lp - 1u};
-    for (uint64_t nd : needs) {
-        const SpectrumShape T = spectrum_shape(nd);
-        if (T.M != S.M || T.log_k != S.log_k) return cudaSuccess;
-    }
+    const uint32_t pb = half - ignore;   // rows of P' (0 at the root: P' is not needed there)
+    // One shape serves the level: the largest product's.  A product whose
+    // own shape is smaller runs at it too (exact either way: the shape only
+    // has to cover the coefficients), which pays when the shared forward
+    // transforms save more than the larger inverse costs.  Cost model:
+    // residues transformed, M * K per row transform; the plain level runs
+    // three transforms per product at each product's own shape.
+    const uint64_t needs[4] = {2ull * lq - 1u, (uint64_t)lr + lq - 1u, (uint64_t)lp + lr - 1u, 2ull * lp - 1u};
+    const uint32_t rows_of[4] = {half, half, half, pb};
+    uint64_t most = 0;
+    for (int i = 0; i < 4; ++i)
+        if (rows_of[i]) most = std::max(most, needs[i]);
+    const SpectrumShape S = spectrum_shape(most);
+    if (S.M == 0) return cudaSuccess;
+    auto cap = [](SpectrumShape s, uint64_t need) { return s.M ? (uint64_t)s.M << s.log_k : need; };
+    uint64_t plain_cost = 0;
+    for (int i = 0; i < 4; ++i) plain_cost += 3ull * rows_of[i] * cap(spectrum_shape(needs[i]), needs[i]);
+    // forward: P_e, Q_e, Q_o, R_e, R_o (half rows each) and P_o (pb rows);
+    // inverse: Q', R1, R2 (half rows each) and P' (pb rows)
+    const uint64_t tuned_cost = (8ull * half + 2ull * pb) * cap(S, most);
+    if (tuned_cost > plain_cost) return cudaSuccess;
     *done = true;
     const NTTPrecomputedTables &tab = context_tables(ctx);
     const uint64_t words = spectrum_words(S, half);
@@ -340,13 +355,14 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
     // odd row count; P_o's row there is left unset and its product unused)
     TRY(stage(pr, "fwd", "P,Q,R columns", n1, half, lp, lq, true, [&]() {
         TRY(fpe.alloc(words));
-        TRY(fpo.alloc(words));
+        if (pb) TRY(fpo.alloc(words));
         TRY(fqo.alloc(words));
         TRY(fqe.alloc(words));
         TRY(fre.alloc(words));
         TRY(fro.alloc(words));
-        spectrum_forward(tab, S, pb, P_even.data, P_even.stride, lp, fpe.p, P_odd.data, P_odd.stride, lp, fpo.p,
-                         false);
+        if (pb)
+            spectrum_forward(tab, S, pb, P_even.data, P_even.stride, lp, fpe.p, P_odd.data, P_odd.stride, lp,
+                             fpo.p, false);
         if (pb < half)
             spectrum_forward(tab, S, 1u, P_even.data + (size_t)pb * P_even.stride, P_even.stride, lp,
                              fpe.p + spectrum_words(S, pb), nullptr, 0, 0, nullptr, false);
@@ -354,8 +370,8 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
                          false);
         spectrum_forward(tab, S, half, R_even.data, R_even.stride, lr, fre.p, R_odd.data, R_odd.stride, lr, fro.p,
                          false);
-        // the four products' row passes in one kernel
-        spectrum_level_rows(tab, S, half, fpe.p, fpo.p, fro.p, fqo.p, fqe.p, fre.p);
+        // the four products' row passes in one kernel (three without P')
+        spectrum_level_rows(tab, S, half, fpe.p, pb ? fpo.p : nullptr, fro.p, fqo.p, fqe.p, fre.p);
         fpe.reset();
         fqo.reset();
         return cudaGetLastError();
@@ -368,11 +384,16 @@ static cudaError_t tuned_level(BatchMPContext *ctx, Profiler *pr, uint32_t n, ui
             return cudaGetLastError();
         });
     };
-    Pn = BatchMPArray{nullptr, 2u * lp, pb, 2u * lp};
-    TRY(pn.alloc((size_t)pb * Pn.stride));
-    Pn.data = pn.p;
-    TRY(finish("P", pb, fpo, Pn.data, Pn.length, lp, lp));
-    TRY(p_compact(ctx, pr, Pn, "P", n1));
+    if (pb) {
+        Pn = BatchMPArray{nullptr, 2u * lp, pb, 2u * lp};
+        TRY(pn.alloc((size_t)pb * Pn.stride));
+        Pn.data = pn.p;
+        TRY(finish("P", pb, fpo, Pn.data, Pn.length, lp, lp));
+        TRY(p_compact(ctx, pr, Pn, "P", n1));
+    } else {
+        pn.reset();
+        Pn = BatchMPArray{nullptr, 0, 0, 0};
+    }
     Qn = BatchMPArray{nullptr, 2u * lq, half, 2u * lq};
     TRY(qn.alloc((size_t)half * Qn.stride));
     Qn.data = qn.p;
@@ -767,8 +788,60 @@ static cudaError_t tree_run(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &
 // sqrt(10005) Pell iteration (pi_bs_gpu.cu:1346-1522): (p, q) <- (p^2 +
 // 10005 q^2, 2pq) from (4001, 40) while 7.5 * 2^k < digits.
 // ---------------------------------------------------------------------------
+// One Pell step in the tuned form: the same P' = P^2 + 10005 Q^2 and
+// Q' = 2 P Q from shared transforms.  P and Q are transformed once, and so
+// is 10005 Q (one small multiply), and P' is the spectral sum
+// P P + (10005 Q) Q: three forward and two inverse transforms instead of
+// four and three, and no separate 10005 x, addition or intermediate
+// compaction passes.  Both results are compacted, as in the plain step, so
+// the lengths (and every later operation) are the plain step's.
+// *done = false (nothing issued) below the shared-transform sizes.
+static cudaError_t sqrt_step_tuned(BatchMPContext *ctx, Profiler *pr, uint32_t sd, const BatchMPArray &P,
+                                   const BatchMPArray &Q, Buf &np, BatchMPArray &NP, Buf &nq, BatchMPArray &NQ,
+                                   bool *done) {
+    *done = false;
+    const uint32_t lp = P.length, lq = Q.length;
+    const uint32_t npl = std::max(2u * lp, 2u * lq + 1u) + 1u;   // P^2 + 10005 Q^2 < 2^(32 (npl - 1) + 1)
+    const SpectrumShape S = spectrum_shape(std::max<uint64_t>(npl - 1u, (uint64_t)lp + lq - 1u));
+    const uint32_t la[2] = {lp, lq + 1u}, lb[2] = {lp, lq};
+    if (S.M == 0 || !spectrum_sum_fits(la, lb, 2)) return cudaSuccess;
+    *done = true;
+    const NTTPrecomputedTables &tab = context_tables(ctx);
+    const uint64_t words = spectrum_words(S, 1u);
+    Buf q5, fp, fq, fq5, flags;
+    TRY(q5.alloc(lq + 1u));
+    const BatchMPArray Q5{q5.p, lq + 1u, 1, lq + 1u};
+    TRY(p_mul_small(ctx, pr, Q, 10005u, Q5, "10005*Q", sd));
+    TRY(flags.alloc(spectrum_flag_words(1u, std::max(npl, lp + lq))));
+    NP = BatchMPArray{nullptr, npl, 1, npl};
+    TRY(np.alloc(npl));
+    NP.data = np.p;
+    BatchMPArray PQ{nullptr, lp + lq, 1, lp + lq};
+    Buf pq;
+    TRY(pq.alloc(PQ.stride));
+    PQ.data = pq.p;
+    TRY(stage(pr, "mul", "P*P+10005*Q*Q, P*Q", sd, 1, lp, lq, true, [&]() {
+        TRY(fp.alloc(words));
+        TRY(fq.alloc(words));
+        TRY(fq5.alloc(words));
+        spectrum_forward(tab, S, 1, P.data, P.stride, lp, fp.p, Q.data, Q.stride, lq, fq.p);
+        spectrum_forward(tab, S, 1, Q5.data, Q5.stride, Q5.length, fq5.p, nullptr, 0, 0, nullptr);
+        const uint32_t *x2[2] = {fp.p, fq5.p}, *y2[2] = {fp.p, fq.p};
+        spectrum_inverse(tab, S, 1, 2, x2, y2, fq5.p, NP.data, NP.stride, NP.length, flags.p);
+        const uint32_t *x1[1] = {fp.p}, *y1[1] = {fq.p};
+        spectrum_inverse(tab, S, 1, 1, x1, y1, fp.p, PQ.data, PQ.stride, PQ.length, flags.p);
+        return cudaGetLastError();
+    }));
+    TRY(p_compact(ctx, pr, NP, "P", sd));
+    NQ = BatchMPArray{nullptr, PQ.length + 1u, 1, PQ.length + 1u};
+    TRY(nq.alloc(NQ.stride));
+    NQ.data = nq.p;
+    TRY(p_shift(ctx, pr, PQ, NQ, 1, "2*P*Q", sd));
+    return p_compact(ctx, pr, NQ, "Q", sd);
+}
+
 static cudaError_t sqrt_10005(BatchMPContext *ctx, Profiler *pr, int target, Buf &pbuf, BatchMPArray &P,
-                              Buf &qbuf, BatchMPArray &Q) {
+                              Buf &qbuf, BatchMPArray &Q, bool tuned) {
     cudaStream_t st = current_stream();
     TRY(pbuf.alloc(1));
     TRY(qbuf.alloc(1));
@@ -784,6 +857,18 @@ static cudaError_t sqrt_10005(BatchMPContext *ctx, Profiler *pr, int target, Buf
         valid *= 2;
         const uint32_t sd = (uint32_t)valid;
         Buf pq, nq, pp, qq, qq5, np;
+        if (tuned) {
+            BatchMPArray NP, NQ;
+            bool done = false;
+            TRY(sqrt_step_tuned(ctx, pr, sd, P, Q, np, NP, nq, NQ, &done));
+            if (done) {
+                pbuf.swap(np);
+                qbuf.swap(nq);
+                P = NP;
+                Q = NQ;
+                continue;
+            }
+        }
         BatchMPArray PQ{nullptr, P.length + Q.length, 1, P.length + Q.length};
         TRY(pq.alloc(PQ.stride));
         PQ.data = pq.p;
@@ -927,8 +1012,21 @@ static cudaError_t shift_right_large(BatchMPContext *ctx, Profiler *pr, BatchMPA
 // ---------------------------------------------------------------------------
 static const uint64_t kInverseCpuLimit = 32 * 1024;   // pi_bs_gpu.cu:1143
 
+// The tuned form's Newton step shares y's forward transform between x2 y
+// and res1m y (five transforms instead of six) when both products fit one
+// shape at less cost than their own two: returns that shape, else M = 0.
+static SpectrumShape newton_shared_shape(uint32_t lx2, uint32_t lres, uint32_t ly) {
+    const uint64_t n1 = (uint64_t)lx2 + ly - 1u, n2 = (uint64_t)lres + ly - 1u;
+    const SpectrumShape s1 = spectrum_shape(n1), s2 = spectrum_shape(n2), S = spectrum_shape(std::max(n1, n2));
+    const uint32_t la[1] = {std::max(lx2, lres)}, lb[1] = {ly};
+    if (s1.M == 0 || s2.M == 0 || S.M == 0 || !spectrum_sum_fits(la, lb, 1)) return SpectrumShape{0, 0};
+    auto cap = [](SpectrumShape s) { return (uint64_t)s.M << s.log_k; };
+    if (5u * cap(S) >= 3u * (cap(s1) + cap(s2))) return SpectrumShape{0, 0};
+    return S;
+}
+
 static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPArray x, uint64_t L, Buf &ybuf,
-                                     BatchMPArray &y_out, uint32_t digits) {
+                                     BatchMPArray &y_out, uint32_t digits, bool tuned) {
     cudaStream_t st = current_stream();
     std::vector<uint64_t> levels{L};
     while (levels.back() > kInverseCpuLimit) {
@@ -980,9 +1078,26 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
         BatchMPArray x2 = subview(x, (uint32_t)((L - L2) >> 6), (uint32_t)(m >> 5));
         BatchMPArray y1 = subview(y_out, (uint32_t)((L - L1) >> 6), y_out.length - (uint32_t)((L - L1) >> 6));
         BatchMPArray x2y1{res2_base, x2.length + y1.length, 1, x2.length + y1.length};
-        TRY(p_mul(ctx, pr, x2, y1, x2y1, "x2*y", dg));
         BatchMPArray res1m{res.data - (uint32_t)(m >> 5), res.length + (uint32_t)(m >> 5) + 1u, 1,
                            res.length + (uint32_t)(m >> 5) + 1u};
+        const SpectrumShape S =
+            tuned ? newton_shared_shape(x2.length, res1m.length, y1.length) : SpectrumShape{0, 0};
+        Buf fy, fz, flags;
+        if (S.M) {
+            const NTTPrecomputedTables &tab = context_tables(ctx);
+            TRY(fy.alloc(spectrum_words(S, 1u)));
+            TRY(fz.alloc(spectrum_words(S, 1u)));
+            TRY(flags.alloc(spectrum_flag_words(1u, std::max(x2y1.length, res1m.length + y1.length))));
+            TRY(stage(pr, "mul", "x2*y", dg, 1, x2.length, y1.length, true, [&]() {
+                spectrum_forward(tab, S, 1, x2.data, x2.stride, x2.length, fz.p, y1.data, y1.stride, y1.length,
+                                 fy.p);
+                const uint32_t *xs[1] = {fz.p}, *ys[1] = {fy.p};
+                spectrum_inverse(tab, S, 1, 1, xs, ys, fz.p, x2y1.data, x2y1.stride, x2y1.length, flags.p);
+                return cudaGetLastError();
+            }));
+        } else {
+            TRY(p_mul(ctx, pr, x2, y1, x2y1, "x2*y", dg));
+        }
         TRY(p_sub(ctx, pr, res1m, x2y1, res1m, "res1_m", dg));
         uint32_t top = 0u;
         TRY(cudaMemcpyAsync(&top, res1m.data + res1m.length - 1, 4, cudaMemcpyDeviceToHost, st));
@@ -993,7 +1108,19 @@ static cudaError_t recursive_inverse(BatchMPContext *ctx, Profiler *pr, BatchMPA
             TRY(p_sub(ctx, pr, BatchMPArray{res1m.data, 0, 1, 0}, res1m, res1m, "res1_m_neg", dg));
         }
         BatchMPArray res2{res2_base, res1m.length + y1.length, 1, res1m.length + y1.length};
-        TRY(p_mul(ctx, pr, res1m, y1, res2, "res2*y", dg));
+        if (S.M) {
+            const NTTPrecomputedTables &tab = context_tables(ctx);
+            TRY(stage(pr, "mul", "res2*y", dg, 1, res1m.length, y1.length, true, [&]() {
+                spectrum_forward(tab, S, 1, res1m.data, res1m.stride, res1m.length, fz.p, nullptr, 0, 0, nullptr);
+                const uint32_t *xs[1] = {fz.p}, *ys[1] = {fy.p};
+                spectrum_inverse(tab, S, 1, 1, xs, ys, fz.p, res2.data, res2.stride, res2.length, flags.p);
+                return cudaGetLastError();
+            }));
+            fy.reset();
+            fz.reset();
+        } else {
+            TRY(p_mul(ctx, pr, res1m, y1, res2, "res2*y", dg));
+        }
         const uint32_t y2len = res2.length - (uint32_t)((L2 - m * 2) >> 5);
         BatchMPArray y2{y2_base, y2len, 1, y2len};
         TRY(shift_right_large(ctx, pr, res2, L2 - m * 2u, y2, "y2", dg));
@@ -1091,7 +1218,7 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     BatchMPArray Rt{Rs.data + extra, Rs.length - (uint32_t)extra, 1, Rs.length - (uint32_t)extra};
     Buf p15b, q15b;
     BatchMPArray P15, Q15;
-    TRY(sqrt_10005(ctx, pr, target, p15b, P15, q15b, Q15));
+    TRY(sqrt_10005(ctx, pr, target, p15b, P15, q15b, Q15, tuned));
     Buf pfb, qfb;
     BatchMPArray Pf{nullptr, P15.length + Qt.length, 1, P15.length + Qt.length};
     BatchMPArray Qf{nullptr, Q15.length + Rt.length, 1, Q15.length + Rt.length};
@@ -1122,7 +1249,7 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     const uint64_t inv_bits = (uint64_t)qbits * 2u - 1u;
     Buf invb;
     BatchMPArray inv;
-    TRY(recursive_inverse(ctx, pr, Qtf, inv_bits, invb, inv, (uint32_t)target));
+    TRY(recursive_inverse(ctx, pr, Qtf, inv_bits, invb, inv, (uint32_t)target, tuned));
     qfb.reset();
     Buf rpb;
     BatchMPArray RP{nullptr, Ptf.length + inv.length, 1, Ptf.length + inv.length};

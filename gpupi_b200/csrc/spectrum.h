@@ -60,7 +60,7 @@ void spectrum_inverse(const NTTPrecomputedTables &tables, SpectrumShape s, uint3
 // One merge level's row products from six column-transformed operands
 // (spectrum_forward with rows = false): P' = P_e P_o into Fpo, R2 = P_e R_o
 // into Fro, Q' = Q_e Q_o into Fqe, R1 = R_e Q_o into Fre, each after its
-// inverse row pass; N rows of shape s.
+// inverse row pass; N rows of shape s.  Fpo null: no P' (five operands).
 void spectrum_level_rows(const NTTPrecomputedTables &tables, SpectrumShape s, uint32_t N, uint32_t *Fpe,
                          uint32_t *Fpo, uint32_t *Fro, uint32_t *Fqo, uint32_t *Fqe, uint32_t *Fre);
 
