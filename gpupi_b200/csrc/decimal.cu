@@ -19,14 +19,13 @@
 #include "batch_decimal_naive.h"
 #include "batch_shift.h"
 #include "convert_decimal.h"
+#include "pi_engine.h"
 
 #include <math.h>
 #include <new>
 #include <vector>
 
 namespace gpupi {
-
-cudaError_t mul_tuned(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 
 constexpr uint32_t kTen9 = 1000000000u;
 
@@ -306,80 +305,87 @@ void convert_decimal_release_powers(ConvertDecimalPowerTable *table) {
     table->levels = 0u;
 }
 
-cudaError_t convert_decimal_equal_split(BatchMPContext *ctx, BatchMPArray input, uint32_t input_bits,
-                                        uint32_t total_digits, uint32_t leaf_digits,
-                                        const ConvertDecimalPowerTable *table, char *output_digits) {
-    if (ctx == nullptr || output_digits == nullptr || input.batch_size != 1u || input.data == nullptr)
-        return cudaErrorInvalidValue;
-    const uint32_t levels = levels_for_shape(total_digits, leaf_digits);
-    if (levels == UINT32_MAX || table == nullptr || table->leaf_digits != leaf_digits ||
-        table->levels != levels)
-        return cudaErrorInvalidValue;
-    cudaStream_t st = current_stream();
+namespace gpupi {
 
-    std::vector<uint32_t> digs(levels + 1), bits(levels + 1), limbs(levels + 1);
-    digs[0] = total_digits;
-    bits[0] = input_bits;
-    limbs[0] = input.length;
+// Level sizes of one conversion (convert_decimal.cu:285-330): digits, bits
+// and limbs of a row at each level.
+struct ConvertPlan {
+    uint32_t levels;
+    std::vector<uint32_t> digs, bits, limbs;
+};
+
+static ConvertPlan convert_plan(uint32_t levels, uint32_t total_digits, uint32_t input_bits, uint32_t input_len) {
+    ConvertPlan p{levels, std::vector<uint32_t>(levels + 1), std::vector<uint32_t>(levels + 1),
+                  std::vector<uint32_t>(levels + 1)};
+    p.digs[0] = total_digits;
+    p.bits[0] = input_bits;
+    p.limbs[0] = input_len;
     for (uint32_t l = 1; l <= levels; ++l) {
-        digs[l] = digs[l - 1] >> 1;
-        bits[l] = bits_for_digits(digs[l]);
-        limbs[l] = (bits[l] + 31u) / 32u;
+        p.digs[l] = p.digs[l - 1] >> 1;
+        p.bits[l] = bits_for_digits(p.digs[l]);
+        p.limbs[l] = (p.bits[l] + 31u) / 32u;
     }
+    return p;
+}
 
-    // Buffers reused across levels: two row sets (ping/pong), mantissa, product.
-    size_t max_rows_words = 0, max_mant = 0, max_prod = 0;
-    for (uint32_t l = 0; l < levels; ++l) {
-        const size_t rows = (size_t)1 << l;
-        max_rows_words = std::max(max_rows_words, rows * 2 * limbs[l + 1]);
-        const uint32_t mant_len = (bits[l] - digs[l + 1] + 31u) / 32u;
-        max_mant = std::max(max_mant, rows * mant_len);
-        max_prod = std::max(max_prod, rows * (mant_len + table->powers[levels - 1 - l].length));
-    }
+// Buffers of levels [l0, l1) for `rows0` rows at level l0: two row sets
+// (ping / pong), the mantissas and the products.
+struct LevelBufs {
     DevBuf ping, pong, mant, prod;
-    BatchMPArray current = input;
-    if (levels == 0u) {
-        const uint32_t need = bits_for_digits(total_digits);
-        const uint32_t nl = (need + 31u) / 32u;
-        if (input_bits < need) return cudaErrorInvalidValue;
-        cudaError_t err = ping.alloc(nl);
-        if (err != cudaSuccess) return err;
-        cudaMemsetAsync(ping.p, 0, (size_t)nl * 4, st);
-        // single row: dst row index 2*0+0 = 0
-        extract_shifted(input, ping.p, nl, nl, 1u, input_bits - need, 0u);
-        current = BatchMPArray{ping.p, nl, 1u, nl};
-    } else {
-        cudaError_t err = ping.alloc(max_rows_words);
-        if (err == cudaSuccess) err = pong.alloc(max_rows_words);
+    cudaError_t alloc(const ConvertPlan &p, const ConvertDecimalPowerTable *table, uint32_t l0, uint32_t l1,
+                      size_t rows0) {
+        size_t rows_words = 0, max_mant = 0, max_prod = 0;
+        for (uint32_t l = l0; l < l1; ++l) {
+            const size_t rows = rows0 << (l - l0);
+            rows_words = std::max(rows_words, rows * 2 * p.limbs[l + 1]);
+            const uint32_t mant_len = (p.bits[l] - p.digs[l + 1] + 31u) / 32u;
+            max_mant = std::max(max_mant, rows * mant_len);
+            max_prod = std::max(max_prod, rows * (mant_len + table->powers[p.levels - 1 - l].length));
+        }
+        cudaError_t err = ping.alloc(rows_words);
+        if (err == cudaSuccess) err = pong.alloc(rows_words);
         if (err == cudaSuccess) err = mant.alloc(max_mant);
         if (err == cudaSuccess) err = prod.alloc(max_prod);
-        if (err != cudaSuccess) return err;
-        DevBuf *bufs[2] = {&ping, &pong};
-        for (uint32_t l = 0; l < levels; ++l) {
-            const uint32_t d = digs[l + 1];
-            const uint32_t cb = bits[l + 1];
-            const uint32_t B = bits[l];
-            if (current.length < limbs[l]) return cudaErrorInvalidValue;
-            if (B <= d || B < cb) return cudaErrorInvalidValue;
-            const uint32_t rows = current.batch_size;
-            const uint32_t nl = limbs[l + 1];
-            uint32_t *next = bufs[l & 1]->p;
-            // every child limb is written by the two extractions below
-            extract_shifted(current, next, nl, nl, rows, B - cb, 0u);
-            const uint32_t mant_bits = B - d;
-            const uint32_t mant_len = (mant_bits + 31u) / 32u;
-            extract_low(current, mant.p, mant_len, mant_len, rows, mant_bits);
-            const BatchMPArray &pw = table->powers[levels - 1 - l];
-            BatchMPArray mA{mant.p, mant_len, rows, mant_len};
-            BatchMPArray pB{pw.data, pw.length, rows, 0u};
-            BatchMPArray pC{prod.p, mant_len + pw.length, rows, mant_len + pw.length};
-            err = mul_tuned(ctx, mA, pB, pC);
-            if (err != cudaSuccess) return err;
-            extract_shifted(pC, next, nl, nl, rows, mant_bits - cb, 1u);
-            current = BatchMPArray{next, nl, rows * 2u, nl};
-        }
+        return err;
     }
-    const uint32_t leaf_bits = (levels == 0u) ? bits_for_digits(total_digits) : bits[levels];
+};
+
+// Levels [l0, l1) on every row of `current` (convert_decimal.cu:331-430):
+// row r becomes rows 2r (high child) and 2r + 1 (low child).  Rows are
+// independent, so any contiguous range of a level's rows can run alone.
+static cudaError_t convert_levels(BatchMPContext *ctx, BatchMPArray &current, const ConvertPlan &p,
+                                  const ConvertDecimalPowerTable *table, uint32_t l0, uint32_t l1, LevelBufs &b) {
+    DevBuf *bufs[2] = {&b.ping, &b.pong};
+    for (uint32_t l = l0; l < l1; ++l) {
+        const uint32_t d = p.digs[l + 1];
+        const uint32_t cb = p.bits[l + 1];
+        const uint32_t B = p.bits[l];
+        if (current.length < p.limbs[l]) return cudaErrorInvalidValue;
+        if (B <= d || B < cb) return cudaErrorInvalidValue;
+        const uint32_t rows = current.batch_size;
+        const uint32_t nl = p.limbs[l + 1];
+        uint32_t *next = bufs[(l - l0) & 1]->p;
+        // every child limb is written by the two extractions below
+        extract_shifted(current, next, nl, nl, rows, B - cb, 0u);
+        const uint32_t mant_bits = B - d;
+        const uint32_t mant_len = (mant_bits + 31u) / 32u;
+        extract_low(current, b.mant.p, mant_len, mant_len, rows, mant_bits);
+        const BatchMPArray &pw = table->powers[p.levels - 1 - l];
+        BatchMPArray mA{b.mant.p, mant_len, rows, mant_len};
+        BatchMPArray pB{pw.data, pw.length, rows, 0u};
+        BatchMPArray pC{b.prod.p, mant_len + pw.length, rows, mant_len + pw.length};
+        const cudaError_t err = mul_tuned(ctx, mA, pB, pC);
+        if (err != cudaSuccess) return err;
+        extract_shifted(pC, next, nl, nl, rows, mant_bits - cb, 1u);
+        current = BatchMPArray{next, nl, rows * 2u, nl};
+    }
+    return cudaSuccess;
+}
+
+// Leaf rows -> digits (convert_decimal.cu:431-474): align each row's
+// leaf_bits at the top of its limbs, then 9 digits per x 10^9 step.
+static cudaError_t convert_leaves(const BatchMPArray &current, uint32_t leaf_bits, uint32_t leaf_digits,
+                                  char *output_digits) {
     const uint32_t align = current.length * 32u - leaf_bits;
     DevBuf aligned;
     cudaError_t err = aligned.alloc((size_t)current.batch_size * current.length);
@@ -388,7 +394,97 @@ cudaError_t convert_decimal_equal_split(BatchMPContext *ctx, BatchMPArray input,
                      current.stride, current.length, (int32_t)align);
     decimal_rows<true>(aligned.p, output_digits, current.batch_size, current.length, current.length,
                        leaf_digits, leaf_digits);
-    err = cudaGetLastError();
+    return cudaGetLastError();
+}
+
+static cudaError_t convert_check(BatchMPContext *ctx, const BatchMPArray &input, uint32_t total_digits,
+                                 uint32_t leaf_digits, const ConvertDecimalPowerTable *table, char *output_digits,
+                                 uint32_t *levels) {
+    if (ctx == nullptr || output_digits == nullptr || input.batch_size != 1u || input.data == nullptr)
+        return cudaErrorInvalidValue;
+    *levels = levels_for_shape(total_digits, leaf_digits);
+    if (*levels == UINT32_MAX || table == nullptr || table->leaf_digits != leaf_digits ||
+        table->levels != *levels)
+        return cudaErrorInvalidValue;
+    return cudaSuccess;
+}
+
+// The conversion with its digits in 2^log_chunks parts: all levels but the
+// last kTailLevels on the whole fraction, then those levels and the leaves
+// for each contiguous range of rows (one part of the digits) after the
+// other; ready(offset, count, user) is called (on the host, in digit order)
+// once each part's digits are issued on the current stream, so that the
+// caller can copy them out while the next parts convert.  Splitting only the
+// last levels keeps the extra launches few and each part's work (about
+// four levels of one part of the rows) longer than its digits' copy.  The
+// digits are those of convert_decimal_equal_split.
+constexpr uint32_t kTailLevels = 4;
+
+cudaError_t convert_decimal_in_parts(BatchMPContext *ctx, BatchMPArray input, uint32_t input_bits,
+                                     uint32_t total_digits, uint32_t leaf_digits,
+                                     const ConvertDecimalPowerTable *table, char *output_digits,
+                                     uint32_t log_chunks, void (*ready)(size_t, size_t, void *), void *user) {
+    uint32_t levels = 0;
+    cudaError_t err = convert_check(ctx, input, total_digits, leaf_digits, table, output_digits, &levels);
+    if (err != cudaSuccess) return err;
+    const uint32_t s = levels > kTailLevels ? levels - kTailLevels : 0u;   // first split level
+    const uint32_t lp = std::min(log_chunks, s);                            // 2^lp parts of 2^(s - lp) rows
+    if (levels == 0u || lp == 0u) {
+        err = convert_decimal_equal_split(ctx, input, input_bits, total_digits, leaf_digits, table, output_digits);
+        if (err == cudaSuccess && ready) ready(0, total_digits, user);
+        return err;
+    }
+    const ConvertPlan p = convert_plan(levels, total_digits, input_bits, input.length);
+    BatchMPArray top = input;
+    LevelBufs tb;
+    err = tb.alloc(p, table, 0u, s, 1u);
+    if (err == cudaSuccess) err = convert_levels(ctx, top, p, table, 0u, s, tb);
+    if (err != cudaSuccess) return err;
+    const uint32_t rows = 1u << (s - lp);
+    const size_t part_digits = (size_t)leaf_digits << (levels - lp);
+    LevelBufs cb;
+    err = cb.alloc(p, table, s, levels, rows);
+    for (uint32_t c = 0; c < (1u << lp) && err == cudaSuccess; ++c) {
+        BatchMPArray cur{top.data + (size_t)c * rows * top.stride, top.length, rows, top.stride};
+        err = convert_levels(ctx, cur, p, table, s, levels, cb);
+        if (err == cudaSuccess) err = convert_leaves(cur, p.bits[levels], leaf_digits, output_digits + c * part_digits);
+        if (err == cudaSuccess && ready) ready(c * part_digits, part_digits, user);
+    }
+    return err;
+}
+
+}  // namespace gpupi
+
+cudaError_t convert_decimal_equal_split(BatchMPContext *ctx, BatchMPArray input, uint32_t input_bits,
+                                        uint32_t total_digits, uint32_t leaf_digits,
+                                        const ConvertDecimalPowerTable *table, char *output_digits) {
+    uint32_t levels = 0;
+    cudaError_t err = convert_check(ctx, input, total_digits, leaf_digits, table, output_digits, &levels);
+    if (err != cudaSuccess) return err;
+    cudaStream_t st = current_stream();
+    BatchMPArray current = input;
+    uint32_t leaf_bits = 0;
+    if (levels == 0u) {
+        const uint32_t need = bits_for_digits(total_digits);
+        const uint32_t nl = (need + 31u) / 32u;
+        if (input_bits < need) return cudaErrorInvalidValue;
+        DevBuf one;
+        err = one.alloc(nl);
+        if (err != cudaSuccess) return err;
+        cudaMemsetAsync(one.p, 0, (size_t)nl * 4, st);
+        // single row: dst row index 2*0+0 = 0
+        extract_shifted(input, one.p, nl, nl, 1u, input_bits - need, 0u);
+        current = BatchMPArray{one.p, nl, 1u, nl};
+        err = convert_leaves(current, need, leaf_digits, output_digits);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+        return err;
+    }
+    const ConvertPlan p = convert_plan(levels, total_digits, input_bits, input.length);
+    LevelBufs b;
+    err = b.alloc(p, table, 0u, levels, 1u);
+    if (err == cudaSuccess) err = convert_levels(ctx, current, p, table, 0u, levels, b);
+    leaf_bits = p.bits[levels];
+    if (err == cudaSuccess) err = convert_leaves(current, leaf_bits, leaf_digits, output_digits);
     if (err == cudaSuccess) err = cudaStreamSynchronize(st);
     return err;
 }

@@ -1333,6 +1333,71 @@ static cudaError_t stream_digits(const char *d_digits, size_t total, const PiReq
     return err;
 }
 
+// Host copies of the digits while they are converted: the conversion runs
+// in parts (convert_decimal_in_parts) and each part's digits go to the
+// caller's buffer on a copy stream once the part is done.  A part's copy is
+// issued when the next part has been issued, so that a copy into pageable
+// memory (which returns only when done) never keeps the GPU waiting.
+struct DigitCopies {
+    cudaStream_t st = nullptr, copy = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    const char *src = nullptr;
+    char *dst = nullptr;
+    size_t want = 0, pend_off = 0, pend_n = 0;
+    int parts = 0;
+    bool pending = false;
+    cudaError_t err = cudaSuccess;
+
+    cudaError_t open(cudaStream_t s) {
+        st = s;
+        cudaError_t e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking);
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+        return e;
+    }
+    void issue_pending() {
+        if (!pending || err != cudaSuccess) return;
+        pending = false;
+        if (pend_off >= want) return;
+        const size_t n = std::min(pend_n, want - pend_off);
+        err = cudaStreamWaitEvent(copy, ev[(parts - 1) & 1], 0);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(dst + pend_off, src + pend_off, n, cudaMemcpyDeviceToHost, copy);
+        note_d2h(n);
+    }
+    static void ready(size_t off, size_t n, void *user) {
+        DigitCopies &d = *static_cast<DigitCopies *>(user);
+        if (d.err != cudaSuccess) return;
+        d.err = cudaEventRecord(d.ev[d.parts & 1], d.st);   // this part's digits are issued before it
+        d.issue_pending();                                   // the previous part's copy
+        ++d.parts;
+        d.pend_off = off;
+        d.pend_n = n;
+        d.pending = true;
+    }
+    void drain() {   // wait for the copies issued so far (error paths)
+        if (copy) cudaStreamSynchronize(copy);
+    }
+    cudaError_t finish() {   // the last part's copy, then wait for all
+        issue_pending();
+        if (copy) {
+            const cudaError_t e = cudaStreamSynchronize(copy);
+            if (err == cudaSuccess) err = e;
+        }
+        return err;
+    }
+    ~DigitCopies() {
+        if (copy) {
+            cudaStreamSynchronize(copy);
+            cudaStreamDestroy(copy);
+        }
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+// Parts of the conversion (2^3) when at least this many digits go to the host.
+constexpr uint32_t kCopyPartsMinDigits = 1u << 24;
+constexpr uint32_t kLogCopyParts = 3;
+
 uint32_t prec_limbs_for_digits(uint32_t digits) {
     const uint32_t bits = (uint32_t)((double)digits * 3.322) + 31u;   // pi_bs_gpu.cu:941-944
     return bits / 32u + 1u;
@@ -1417,12 +1482,30 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
         err = stage(&prof, "decimal_powers", "precompute_5pow", levels == 0u ? leaf : (leaf << levels), 1u, levels,
                     leaf, false, [&]() { return convert_decimal_precompute_powers(ctx, &powers, leaf, levels); });
     }
+    // digits for the host: copied part by part while the rest converts
+    const uint32_t want = req.device_only ? 0u : std::min(requested, req.copy_digits);
+    char *dst = req.host_digits;
+    if (want > 0u && !dst) {
+        out.digits.resize(want);
+        dst = &out.digits[0];
+    }
+    const bool in_parts = want >= kCopyPartsMinDigits && !req.profile_stages;
+    DigitCopies copies;
     if (err == cudaSuccess && requested > 0u) {
         err = scratch_alloc((void **)&d_digits, convert);
+        if (err == cudaSuccess && in_parts) {
+            err = copies.open(st);
+            copies.src = d_digits;
+            copies.dst = dst;
+            copies.want = want;
+        }
         if (err == cudaSuccess) {
             BatchMPArray frac = subview(RET, 0u, std::min<uint32_t>(prec, RET.length));
             err = stage(&prof, "decimal_convert", "equal_split", convert, frac.batch_size, frac.length, leaf, false,
                         [&]() {
+                            if (in_parts)
+                                return convert_decimal_in_parts(ctx, frac, prec * 32u, convert, leaf, &powers,
+                                                                d_digits, kLogCopyParts, DigitCopies::ready, &copies);
                             return convert_decimal_equal_split(ctx, frac, prec * 32u, convert, leaf, &powers,
                                                                d_digits);
                         });
@@ -1439,13 +1522,8 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
             err = cudaMemcpyAsync(out.ret.data(), RET.data, (size_t)RET.length * 4, cudaMemcpyDeviceToHost, st);
             note_d2h((size_t)RET.length * 4);
         }
-        const uint32_t want = std::min(requested, req.copy_digits);
-        if (err == cudaSuccess && want > 0u) {
-            char *dst = req.host_digits;
-            if (!dst) {
-                out.digits.resize(want);
-                dst = &out.digits[0];
-            }
+        if (err == cudaSuccess && want > 0u && in_parts) err = copies.finish();
+        if (err == cudaSuccess && want > 0u && !in_parts) {
             err = cudaMemcpyAsync(dst, d_digits, want, cudaMemcpyDeviceToHost, st);
             note_d2h(want);
         }
@@ -1466,6 +1544,7 @@ cudaError_t pi_run(const PiRequest &req, PiOutput &out) {
     }
     if (ret_ready) cudaEventDestroy(ret_ready);
     out.stages = prof.entries;
+    copies.drain();
     scratch_free(d_digits);
     convert_decimal_release_powers(&powers);
     retb.reset();

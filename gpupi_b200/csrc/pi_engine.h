@@ -9,6 +9,8 @@
 #include "batch_arith.h"
 #include "batch_mul_ntt.h"
 
+struct ConvertDecimalPowerTable;
+
 namespace gpupi {
 
 struct StageEntry {
@@ -59,6 +61,14 @@ struct PiOutput {
 cudaError_t pi_run(const PiRequest &req, PiOutput &out);
 uint32_t round_up_decimal_digits(uint32_t requested, uint32_t *leaf_out);
 uint32_t prec_limbs_for_digits(uint32_t digits);
+
+// convert_decimal_equal_split in 2^log_chunks parts, each part's digits
+// announced to ready(offset, count, user) as soon as they are issued on the
+// current stream (decimal.cu).
+cudaError_t convert_decimal_in_parts(BatchMPContext *ctx, BatchMPArray input, uint32_t input_bits,
+                                     uint32_t total_digits, uint32_t leaf_digits,
+                                     const ConvertDecimalPowerTable *table, char *output_digits,
+                                     uint32_t log_chunks, void (*ready)(size_t, size_t, void *), void *user);
 
 cudaError_t mul_ntt_direct(BatchMPContext *ctx, BatchMPArray A, BatchMPArray B, BatchMPArray C);
 // batch_mp_mul with this library's schoolbook/NTT crossover (school_max()).
