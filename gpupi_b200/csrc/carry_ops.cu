@@ -15,7 +15,8 @@
 // zero-extended to L_c" semantics directly.
 //
 // Launch shapes (all sm_100a, no inter-CTA waiting):
-//   * thread per row   - tiny rows (L_c <= 8) in huge batches;
+//   * lanes per row    - short rows (L_c <= 32) in huge batches: 8, 16 or
+//                        32 lanes per row, one ballot pair;
 //   * warp per row     - 32-limb groups resolved with two ballots and one
 //                        64-bit add (common.cuh), carry kept warp-uniform;
 //   * tiles + fix-up   - long rows: each CTA owns a 4096-limb tile, writes its
@@ -105,29 +106,32 @@ struct GenShiftTwo {
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
-template <class Gen, bool SUB>
-__global__ void carry_thread_rows(Gen gen, uint32_t *C, uint64_t sC, uint32_t N, uint32_t Lc) {
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < N;
-         row += gridDim.x * blockDim.x) {
-        uint32_t c = 0u;
-        uint32_t *out = C + row * sC;
-        for (uint32_t j = 0; j < Lc; ++j) {
-            uint32_t x, y;
-            gen(row, j, x, y);
-            uint32_t s;
-            if (SUB) {
-                const uint32_t d = x - y;
-                const uint32_t b1 = x < y;
-                s = d - c;
-                c = b1 | (d < c);
-            } else {
-                const uint32_t t = x + y;
-                const uint32_t c1 = t < x;
-                s = t + c;
-                c = c1 | (s < t);
-            }
-            out[j] = s;
-        }
+// G lanes per row (G = 8, 16, 32; L_c <= G), 32 / G rows per warp: the
+// short rows of the splitting tree's lower levels (millions of 6..32-limb
+// rows) with whole groups of lanes reading and writing each row's limbs
+// contiguously.
+template <class Gen, bool SUB, int G>
+__global__ void carry_seg_rows(Gen gen, uint32_t *C, uint64_t sC, uint32_t N, uint32_t Lc) {
+    constexpr uint32_t kMask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+    const uint32_t lane = lane_id();
+    const uint32_t grp = lane / G, gl = lane % G;
+    const uint32_t warps_per_cta = blockDim.x >> 5;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * warps_per_cta + (threadIdx.x >> 5);
+    const uint64_t nwarps = (uint64_t)gridDim.x * warps_per_cta;
+    // the whole warp runs every iteration (ballots); rows past N do nothing
+    for (uint64_t base = gwarp * (32 / G); base < N; base += nwarps * (32 / G)) {
+        const uint64_t row = base + grp;
+        const bool valid = row < N && gl < Lc;
+        uint32_t x = 0u, y = 0u;
+        if (valid) gen((uint32_t)row, gl, x, y);
+        bool g, p;
+        const uint32_t s = raw_limb<SUB>(x, y, g, p);
+        if (!valid) g = p = false;
+        const uint32_t gm = (__ballot_sync(0xffffffffu, g) >> (grp * G)) & kMask;
+        const uint32_t pm = (__ballot_sync(0xffffffffu, p) >> (grp * G)) & kMask;
+        const GroupCarry gc = resolve_group_n(gm, pm, 0u, G);
+        const uint32_t r = apply_carry<SUB>(s, (gc.carry_in_mask >> gl) & 1u);
+        if (valid) C[row * sC + gl] = r;
     }
 }
 
@@ -255,10 +259,10 @@ carry_tiles(Gen gen, uint32_t *C, uint64_t sC, uint32_t Lc, uint32_t tiles_per_r
 // ---------------------------------------------------------------------------
 // Dispatch
 // ---------------------------------------------------------------------------
-enum class CarryPlan { Thread, Warp, Tiles };
+enum class CarryPlan { Lanes, Warp, Tiles };
 
 static CarryPlan plan_for(uint32_t N, uint32_t Lc) {
-    if (Lc <= 8u && N >= 2048u) return CarryPlan::Thread;
+    if (Lc <= 32u && N >= 2048u) return CarryPlan::Lanes;
     if (Lc <= kTileSpan || (uint64_t)N >= (uint64_t)kNumSMs * 64u) return CarryPlan::Warp;
     return CarryPlan::Tiles;
 }
@@ -276,8 +280,14 @@ static void run_carry(const Gen &gen, uint32_t *C, uint32_t N, uint32_t Lc, uint
     cudaStream_t st = current_stream();
     const CarryPlan plan = plan_for(N, Lc);
     KernelTimed kt("carry_chain", 4.0 * N * (gen.read_limbs(Lc) + (double)Lc));
-    if (plan == CarryPlan::Thread) {
-        carry_thread_rows<Gen, SUB><<<grid_for(N, 128), 128, 0, st>>>(gen, C, sC, N, Lc);
+    if (plan == CarryPlan::Lanes) {
+        // rows per 256-thread CTA: 8 warps x 32 / G
+        if (Lc <= 8u)
+            carry_seg_rows<Gen, SUB, 8><<<grid_for(N, 32, kNumSMs * 32), 256, 0, st>>>(gen, C, sC, N, Lc);
+        else if (Lc <= 16u)
+            carry_seg_rows<Gen, SUB, 16><<<grid_for(N, 16, kNumSMs * 32), 256, 0, st>>>(gen, C, sC, N, Lc);
+        else
+            carry_seg_rows<Gen, SUB, 32><<<grid_for(N, 8, kNumSMs * 32), 256, 0, st>>>(gen, C, sC, N, Lc);
         GPUPI_LAUNCH_CHECK();
     } else if (plan == CarryPlan::Warp) {
         const unsigned warps = 8;

@@ -4,8 +4,8 @@
 //   * k_school_thread<MA, MB>: one thread per product for operands of at most
 //     MA x MB limbs (the bottom levels of the splitting tree: 3..16-limb rows
 //     in batches of millions).  Register arrays, fully unrolled MACs.
-//   * k_school_warp: one warp per product for L_a + L_b <= 128, eight
-//     products per CTA, carries resolved with one ballot pair.
+//   * k_school_seg<G>: G = 8, 16 or 32 lanes per product for
+//     L_a + L_b <= 4 G (up to 128), carries resolved with one ballot pair.
 //   * k_school_cols: one CTA per product, 64-256 threads x 4 consecutive output
 //     columns.  Each column sum sum_i a_i b_(k-i) is accumulated exactly in a
 //     3-word register with mad.lo.cc / madc.hi.cc / addc (3 instructions per
@@ -65,39 +65,63 @@ __device__ __forceinline__ void mac3(uint32_t &c0, uint32_t &c1, uint32_t &c2, u
 constexpr int kSchoolV = 4;
 constexpr int kSchoolMaxL = 256 * kSchoolV;   // 1024 output limbs
 
-// One warp per product, L_a + L_b <= 128: lane l owns output columns
-// 4l .. 4l+3; carries between lanes are resolved with one ballot pair.
-constexpr int kWarpProducts = 8;   // products (warps) per CTA
+// G lanes per product (G = 8, 16, 32; L_a + L_b <= 4 G): lane l of a group
+// owns output columns 4l .. 4l+3, carries between the group's lanes are
+// resolved with one ballot pair.  32 / G products per warp, so short
+// products (the lower levels of the splitting tree) keep most lanes busy.
+constexpr int kSegWarps = 8;   // warps per CTA
 
-__global__ void __launch_bounds__(32 * kWarpProducts) k_school_warp(const uint32_t *__restrict__ A,
-                                                                    const uint32_t *__restrict__ B,
-                                                                    uint32_t *__restrict__ C, uint32_t N,
-                                                                    uint32_t La, uint32_t Lb, uint64_t sA,
-                                                                    uint64_t sB, uint64_t sC) {
-    __shared__ uint32_t sa[kWarpProducts][128];
-    __shared__ uint32_t sb[kWarpProducts][128 + 128 + 8];
+template <int G>
+__global__ void __launch_bounds__(32 * kSegWarps) k_school_seg(const uint32_t *__restrict__ A,
+                                                               const uint32_t *__restrict__ B,
+                                                               uint32_t *__restrict__ C, uint32_t N,
+                                                               uint32_t La, uint32_t Lb, uint64_t sA,
+                                                               uint64_t sB, uint64_t sC) {
+    constexpr int PW = 32 / G;                    // products per warp
+    constexpr int NP = kSegWarps * PW;            // products per CTA
+    // row pitches: 4G + 1 words for A (the groups' broadcast reads of a_i hit
+    // different banks), 4G + 13 for B (the groups' windows start in
+    // different banks modulo 4)
+    __shared__ uint32_t sa[NP][4 * G + 1];
+    __shared__ uint32_t sb[NP][4 * G + 13];
     const uint32_t lane = lane_id();
     const uint32_t w = threadIdx.x >> 5;
+    const uint32_t grp = lane / G, gl = lane % G;   // group in the warp, lane in the group
+    const uint32_t slot = w * PW + grp;
     const uint32_t kPad = La + 4;
     const uint32_t Lc = La + Lb;
-    for (uint32_t row = blockIdx.x * kWarpProducts + w; row < N; row += gridDim.x * kWarpProducts) {
+    const uint32_t gmask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+    // the whole warp runs every iteration (ballots), rows past N compute zeros
+    for (uint64_t base = ((uint64_t)blockIdx.x * kSegWarps + w) * PW; base < N;
+         base += (uint64_t)gridDim.x * NP) {
+        const uint64_t row = base + grp;
+        const bool valid = row < N;
         const uint32_t *ar = A + row * sA;
         const uint32_t *br = B + row * sB;
-        for (uint32_t i = lane; i < La; i += 32) sa[w][i] = ar[i];
-        for (uint32_t j = lane; j < kPad + Lb + 8; j += 32) sb[w][j] = (j >= kPad && j - kPad < Lb) ? br[j - kPad] : 0u;
+        for (uint32_t i = gl; i < La; i += G) sa[slot][i] = valid ? ar[i] : 0u;
+        for (uint32_t j = gl; j < kPad + Lb + 8; j += G)
+            sb[slot][j] = (valid && j >= kPad && j - kPad < Lb) ? br[j - kPad] : 0u;
         __syncwarp();
-        const uint32_t k0 = lane * kSchoolV;
+        const uint32_t k0 = gl * kSchoolV;
         uint32_t c[kSchoolV][3];
 #pragma unroll
         for (int v = 0; v < kSchoolV; ++v) c[v][0] = c[v][1] = c[v][2] = 0u;
         if (k0 < Lc) {
             const int ilo = max(0, (int)k0 + 1 - (int)Lb);
             const int ihi = min((int)La - 1, (int)k0 + kSchoolV - 1);
+            // window bw[v] = b_(k0 + v - i), slid down one word per step of i:
+            // one shared-memory load per four products
+            const uint32_t *bcol = &sb[slot][kPad + k0];
+            uint32_t bw[kSchoolV];
+#pragma unroll
+            for (int v = 0; v < kSchoolV; ++v) bw[v] = bcol[v - ilo];
             for (int i = ilo; i <= ihi; ++i) {
-                const uint32_t ai = sa[w][i];
-                const uint32_t *bw = &sb[w][kPad + k0 - i];
+                const uint32_t ai = sa[slot][i];
 #pragma unroll
                 for (int v = 0; v < kSchoolV; ++v) mac3(c[v][0], c[v][1], c[v][2], ai, bw[v]);
+#pragma unroll
+                for (int v = kSchoolV - 1; v > 0; --v) bw[v] = bw[v - 1];
+                bw[0] = bcol[-i - 1];
             }
         }
         uint32_t S[kSchoolV + 3];
@@ -106,20 +130,32 @@ __global__ void __launch_bounds__(32 * kWarpProducts) k_school_warp(const uint32
         H[0] = __shfl_up_sync(0xffffffffu, S[kSchoolV], 1);
         H[1] = __shfl_up_sync(0xffffffffu, S[kSchoolV + 1], 1);
         H[2] = __shfl_up_sync(0xffffffffu, S[kSchoolV + 2], 1);
-        if (lane == 0) H[0] = H[1] = H[2] = 0u;
+        if (gl == 0) H[0] = H[1] = H[2] = 0u;
         uint32_t X[kSchoolV];
         const uint32_t g = chunk_add_spill<kSchoolV>(S, H, X);
         bool pp = true;
 #pragma unroll
         for (int v = 0; v < kSchoolV; ++v) pp = pp && (X[v] == 0xffffffffu);
-        const GroupCarry gc = resolve_group(__ballot_sync(0xffffffffu, g != 0u), __ballot_sync(0xffffffffu, pp), 0u);
-        chunk_increment<kSchoolV>(X, (gc.carry_in_mask >> lane) & 1u);
-        uint32_t *cr = C + row * sC;
+        const uint32_t gb = (__ballot_sync(0xffffffffu, g != 0u) >> (grp * G)) & gmask;
+        const uint32_t pb = (__ballot_sync(0xffffffffu, pp) >> (grp * G)) & gmask;
+        const GroupCarry gc = resolve_group_n(gb, pb, 0u, G);
+        chunk_increment<kSchoolV>(X, (gc.carry_in_mask >> gl) & 1u);
+        if (valid) {
+            uint32_t *cr = C + row * sC;
 #pragma unroll
-        for (int v = 0; v < kSchoolV; ++v)
-            if (k0 + v < Lc) cr[k0 + v] = X[v];
+            for (int v = 0; v < kSchoolV; ++v)
+                if (k0 + v < Lc) cr[k0 + v] = X[v];
+        }
         __syncwarp();
     }
+}
+
+template <int G>
+static void launch_seg(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, uint32_t La, uint32_t Lb,
+                       uint64_t sA, uint64_t sB, uint64_t sC, cudaStream_t st) {
+    constexpr int NP = kSegWarps * (32 / G);
+    k_school_seg<G><<<grid_for(N, NP, kNumSMs * 32), 32 * kSegWarps, 0, st>>>(A, B, C, N, La, Lb, sA, sB, sC);
+    count_launch();
 }
 
 // RAGGED: per-product descriptors (rows) give each product's offsets and
@@ -230,10 +266,12 @@ void school_mul(const uint32_t *A, const uint32_t *B, uint32_t *C, uint32_t N, u
         launch_thread<16, 8>(A, B, C, N, La, Lb, sA, sB, sC, st);
     } else if (La <= 16u && Lb <= 16u) {
         launch_thread<16, 16>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else if (La + Lb <= 32u) {
+        launch_seg<8>(A, B, C, N, La, Lb, sA, sB, sC, st);
+    } else if (La + Lb <= 64u) {
+        launch_seg<16>(A, B, C, N, La, Lb, sA, sB, sC, st);
     } else if (La + Lb <= 128u) {
-        k_school_warp<<<grid_for(N, kWarpProducts, kNumSMs * 32), 32 * kWarpProducts, 0, st>>>(A, B, C, N, La, Lb,
-                                                                                            sA, sB, sC);
-        count_launch();
+        launch_seg<32>(A, B, C, N, La, Lb, sA, sB, sC, st);
     } else {
         // one CTA per product, 4 output columns per thread
         const uint32_t g = grid_for(N, 1, kNumSMs * 16);

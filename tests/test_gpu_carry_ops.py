@@ -27,6 +27,9 @@ FIXED = [
     (2, 8192, 8191, 4096, 8192, 8191, 4096),
     (5, 0, 23, 24, 3, 27, 29),
     (5000, 3, 4, 6, 3, 4, 6),
+    (4099, 9, 11, 13, 10, 12, 15),
+    (3001, 16, 16, 16, 16, 16, 17),
+    (2500, 20, 31, 32, 21, 31, 33),
     (1, 100000, 99999, 100001, 100000, 99999, 100001),
 ]
 
@@ -107,7 +110,7 @@ def test_small_ops(ctx, case, op):
 @pytest.mark.parametrize("op", ["shift_add", "shift_sub"])
 def test_shift_addsub(ctx, shift, op):
     rng = np.random.default_rng(5 + shift)
-    for (N, La, Lb, sA, sB) in [(64, 10, 9, 10, 9), (3, 5000, 5100, 5000, 5100)]:
+    for (N, La, Lb, sA, sB) in [(64, 10, 9, 10, 9), (3, 5000, 5100, 5000, 5100), (3000, 6, 9, 12, 9)]:
         Lc = max(La + shift // 32 + 1, Lb) + 1
         A, B, C = rand_buf(rng, N, sA, La), rand_buf(rng, N, sB, Lb), rand_buf(rng, N, Lc, 0)
         dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)

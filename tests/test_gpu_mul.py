@@ -36,13 +36,26 @@ def _check_mul(ctx, N, La, Lb, sA, sB, sC, rng, path="auto", extreme=False):
         assert ref.mul_check(N, A, La, sA, B, Lb, sB, got, sC)
 
 
-@pytest.mark.parametrize("La,Lb", [(1, 1), (3, 3), (4, 3), (6, 4), (8, 8), (12, 5), (16, 16), (17, 16), (21, 16), (64, 64), (65, 64), (150, 50),
+@pytest.mark.parametrize("La,Lb", [(1, 1), (3, 3), (4, 3), (6, 4), (8, 8), (12, 5), (16, 16), (17, 3), (3, 17),
+                                   (20, 12), (31, 1), (17, 16), (21, 16), (64, 64), (65, 64), (150, 50),
                                    (33, 31), (100, 7), (256, 256), (511, 513), (1000, 24)])
 def test_schoolbook(ctx, La, Lb):
     rng = np.random.default_rng(La * 1000 + Lb)
     N = 300 if La + Lb < 64 else 17
     _check_mul(ctx, N, La, Lb, La + 3, Lb + 1, La + Lb + 2, rng, path="naive")
     _check_mul(ctx, 3, La, Lb, La, Lb, La + Lb, rng, path="naive", extreme=True)
+
+
+@pytest.mark.parametrize("La,Lb", [(3, 3), (6, 4), (11, 11), (15, 15), (18, 15), (11, 18), (21, 21), (34, 29),
+                                   (41, 3), (42, 42), (68, 59)])
+def test_schoolbook_many_rows(ctx, La, Lb):
+    """The splitting tree's lower-level shapes in batches of thousands of rows,
+    the operands as every other row of a wider array (the level's even and
+    odd views): every row-tile and lane-group boundary of the kernels."""
+    rng = np.random.default_rng(7 * La + Lb)
+    N = 5003
+    _check_mul(ctx, N, La, Lb, 2 * La, 2 * Lb + 1, La + Lb, rng, path="naive")
+    _check_mul(ctx, 129, La, Lb, La, Lb, La + Lb, rng, path="naive", extreme=True)
 
 
 @pytest.mark.parametrize("La,Lb", [(1, 1), (2, 3), (100, 100), (513, 511), (1000, 1000), (2048, 2048),
