@@ -7,12 +7,15 @@
 // last CTA to finish (ticket counter) moves the result straight into pinned,
 // mapped host memory and re-zeroes the word and the counter, so a call is one
 // launch plus one stream synchronisation — no memset, no device-to-host copy.
-// The two device words belong to the library (one pair per device, zeroed when
-// first created) and return to zero after every call.  Calls are issued on the
-// library's single stream, so they never overlap.
+// The two device words belong to the library (one pair per device and
+// stream, zeroed when first created) and return to zero after every call.
+// Calls on one stream run in order, so a pair is never used by two scans at
+// once; scans on different streams (the splitting tree's graph on its own
+// stream, other work beside it) use different pairs.
 #include "common.cuh"
 #include "batch_bitlength.h"
 
+#include <deque>
 #include <mutex>
 
 namespace gpupi {
@@ -131,31 +134,46 @@ __global__ void __launch_bounds__(256) length_max_rows_kernel(const uint32_t *__
 
 namespace {
 struct LengthState {
+    int dev_id = -1;
+    cudaStream_t stream = nullptr;
     uint32_t *dev = nullptr;            // [0] = max, [1] = ticket counter
     volatile uint32_t *host = nullptr;  // pinned, mapped
     uint32_t *host_dev = nullptr;       // device view of host
 };
-LengthState g_len[64];
+// Entries are never removed: graphs captured on a stream keep their pair's
+// addresses.  A deque keeps them in place as it grows.
+std::deque<LengthState> g_len;
 std::mutex g_len_mu;
 
 LengthState *length_state() {
     int d = 0;
-    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0) return nullptr;
+    const cudaStream_t st = current_stream();
     std::lock_guard<std::mutex> g(g_len_mu);
-    LengthState &s = g_len[d];
-    if (!s.dev) {
+    for (LengthState &e : g_len)
+        if (e.dev_id == d && e.stream == st) return &e;
+    g_len.push_back(LengthState{});
+    LengthState &s = g_len.back();
+    s.dev_id = d;
+    s.stream = st;
+    {
         uint32_t *dev = nullptr;
         void *host = nullptr;
-        if (cudaMalloc(&dev, 2 * sizeof(uint32_t)) != cudaSuccess) return nullptr;
+        if (cudaMalloc(&dev, 2 * sizeof(uint32_t)) != cudaSuccess) {
+            g_len.pop_back();
+            return nullptr;
+        }
         if (cudaMemset(dev, 0, 2 * sizeof(uint32_t)) != cudaSuccess ||
             cudaHostAlloc(&host, sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess) {
             cudaFree(dev);
+            g_len.pop_back();
             return nullptr;
         }
         uint32_t *hd = nullptr;
         if (cudaHostGetDevicePointer((void **)&hd, host, 0) != cudaSuccess) {
             cudaFree(dev);
             cudaFreeHost(host);
+            g_len.pop_back();
             return nullptr;
         }
         cudaDeviceSynchronize();
@@ -193,6 +211,10 @@ static uint32_t length_max(const uint32_t *A, uint32_t *workspace, uint32_t N, u
     note_d2h(sizeof(uint32_t));
     return *s->host;
 }
+
+// Creates the current stream's pair of words ahead of a stream capture (their
+// creation synchronises the device, which a capture does not allow).
+cudaError_t limb_length_prepare() { return length_state() ? cudaSuccess : cudaErrorMemoryAllocation; }
 
 // The limb length of a batch written to device memory (d_out), without a
 // host synchronisation: the same scans, the result stored where one later

@@ -152,9 +152,10 @@ static cudaError_t p_mul(BatchMPContext *ctx, Profiler *pr, BatchMPArray A, Batc
 // them (RECORD); later runs take them from the record and only launch the
 // scans, writing into a device array that is compared with the record once
 // the tree is done (REPLAY).  With no host synchronisation left inside it,
-// the tree can be captured into a CUDA graph (tree_run).
+// the tree can be captured into a CUDA graph (tree_start).
 // ---------------------------------------------------------------------------
 cudaError_t limb_length_to_device(const uint32_t *A, uint32_t N, uint32_t L, uint32_t stride, uint32_t *d_out);
+cudaError_t limb_length_prepare();
 
 enum TreeMode { kTreeDirect = 0, kTreeRecord = 1, kTreeReplay = 2 };
 struct TreeLens {
@@ -587,6 +588,18 @@ cudaStream_t tree_stream(int dev) {
     return s[dev];
 }
 
+// Two events per device: the caller's stream's work before the graph, and
+// the graph's end.
+cudaEvent_t *tree_events(int dev) {
+    static cudaEvent_t evs[64][2] = {};
+    cudaEvent_t *ev = evs[dev & 63];
+    if (!ev[0]) {
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    }
+    return ev;
+}
+
 bool tree_graphs_enabled() {
     const char *e = getenv("GPUPI_TREE_GRAPH");
     return !(e && e[0] == '0');
@@ -604,7 +617,40 @@ void tree_graph_perturb() {
         if (!g.lens.empty() && g.lens[0] > 1u) g.lens[0] -= 1u;
 }
 
+// A second context per caller context for the work that runs beside the
+// tree's graph (the sqrt(10005) iteration): the graph's products use the
+// caller context's workspace, so the side work needs its own.
+static std::mutex g_side_mu;
+static std::vector<std::pair<const BatchMPContext *, BatchMPContext *>> g_sides;
+
+static BatchMPContext *side_context(const BatchMPContext *ctx) {
+    std::lock_guard<std::mutex> l(g_side_mu);
+    for (auto &e : g_sides)
+        if (e.first == ctx) return e.second;
+    BatchMPContext *side = batch_mp_init();
+    if (!side) return nullptr;
+    // the side work's products below the shared-transform sizes: no
+    // workspace growth (a synchronising allocation) while the graph runs
+    if (batch_mp_ensure_workspace(side, batch_mul_ntt_workspace_size(1u, 8192u, 8192u)) != cudaSuccess) {
+        batch_mp_destroy(side);
+        return nullptr;
+    }
+    g_sides.emplace_back(ctx, side);
+    return side;
+}
+
 void pi_forget_context(const BatchMPContext *ctx) {
+    BatchMPContext *side = nullptr;
+    {
+        std::lock_guard<std::mutex> l(g_side_mu);
+        for (auto it = g_sides.begin(); it != g_sides.end(); ++it)
+            if (it->first == ctx) {
+                side = it->second;
+                g_sides.erase(it);
+                break;
+            }
+    }
+    if (side) batch_mp_destroy(side);
     std::lock_guard<std::mutex> l(g_tree_mu);
     for (auto it = g_trees.begin(); it != g_trees.end();) {
         if (it->ctx == ctx) {
@@ -651,6 +697,12 @@ static cudaError_t tree_capture(BatchMPContext *ctx, TreeGraph &g, bool *usable)
     t_tree.lens = &g.lens;
     t_tree.d_check = g.d_check;
     set_current_stream(ts);
+    if (limb_length_prepare() != cudaSuccess) {   // the tree stream's length-scan words, before capturing
+        set_current_stream(st);
+        t_tree = TreeLens{};
+        tree_release(g);
+        return cudaSuccess;
+    }
     scratch_private_begin(g.pool, cap);
     cudaGraph_t graph = nullptr;
     Buf q, r;
@@ -690,8 +742,25 @@ static cudaError_t tree_capture(BatchMPContext *ctx, TreeGraph &g, bool *usable)
     return cudaSuccess;
 }
 
-static cudaError_t tree_run(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &qbuf, BatchMPArray &Q, Buf &rbuf,
-                            BatchMPArray &R, bool tuned) {
+// A tree whose graph was launched and not yet joined: the graph runs on the
+// tree stream while the caller's stream is free for independent work.  The
+// tree's lock is held until the join.
+struct TreeJoin {
+    std::unique_lock<std::mutex> lock;
+    TreeGraph *g = nullptr;   // null: the tree has already run (directly)
+    BatchMPContext *ctx = nullptr;
+    Profiler *pr = nullptr;
+    uint32_t N = 0;
+    bool tuned = false;
+};
+
+// Starts the tree: a captured graph is launched on the tree stream after
+// the caller's stream's work and left running (tj.g set; tree_join orders
+// the caller's stream after it and checks the lengths); otherwise the tree
+// runs directly, recording or capturing its graph on the way.
+static cudaError_t tree_start(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &qbuf, BatchMPArray &Q,
+                              Buf &rbuf, BatchMPArray &R, bool tuned, TreeJoin &tj) {
+    tj = TreeJoin{};
     if (!tree_graphs_enabled() || (pr && pr->on) || kernel_timer_enabled())
         return binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
     int dev = 0;
@@ -744,23 +813,34 @@ static cudaError_t tree_run(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &
         }
         ++g_tree_stats.captured;
     }
-    // launch the graph after the caller's stream's work, and the caller's
-    // stream after it
+    // launch the graph after the caller's stream's work
     cudaStream_t st = current_stream(), ts = tree_stream(dev);
-    static cudaEvent_t evs[64][2] = {};
-    cudaEvent_t *ev = evs[dev & 63];
-    if (!ev[0]) {
-        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
-    }
+    cudaEvent_t *ev = tree_events(dev);
     cudaError_t err = cudaEventRecord(ev[0], st);
     if (err == cudaSuccess) err = cudaStreamWaitEvent(ts, ev[0], 0);
     if (err == cudaSuccess) err = cudaGraphLaunch(g->exec, ts);
     if (err == cudaSuccess) err = cudaEventRecord(ev[1], ts);
-    if (err == cudaSuccess) err = cudaStreamWaitEvent(st, ev[1], 0);
     if (err != cudaSuccess) return err;
     add_launches(g->launches);
-    // the lengths the device found, against the schedule the graph used
+    tj.lock = std::move(lock);
+    tj.g = g;
+    tj.ctx = ctx;
+    tj.pr = pr;
+    tj.N = N;
+    tj.tuned = tuned;
+    return cudaSuccess;
+}
+
+// Orders the caller's stream after a launched graph and checks the lengths
+// the device found against the schedule the graph used (a disagreement,
+// never expected, runs the tree directly and records it again).
+static cudaError_t tree_join(TreeJoin &tj, Buf &qbuf, BatchMPArray &Q, Buf &rbuf, BatchMPArray &R) {
+    TreeGraph *g = tj.g;
+    if (!g) return cudaSuccess;
+    tj.g = nullptr;
+    cudaStream_t st = current_stream();
+    cudaError_t err = cudaStreamWaitEvent(st, tree_events(g->dev)[1], 0);
+    if (err != cudaSuccess) return err;
     std::vector<uint32_t> seen(g->lens.size());
     if (!seen.empty()) {
         err = cudaMemcpyAsync(seen.data(), g->d_check, seen.size() * 4, cudaMemcpyDeviceToHost, st);
@@ -773,14 +853,15 @@ static cudaError_t tree_run(BatchMPContext *ctx, Profiler *pr, uint32_t N, Buf &
         tree_release(*g);
         g->lens.clear();
         g->state = 0;
-        lock.unlock();
-        return binary_split(ctx, pr, N, qbuf, Q, rbuf, R, tuned);
+        tj.lock.unlock();
+        return binary_split(tj.ctx, tj.pr, tj.N, qbuf, Q, rbuf, R, tj.tuned);
     }
     ++g_tree_stats.replayed;
     qbuf.reset();
     rbuf.reset();
     Q = BatchMPArray{g->q, g->lq, 1, g->lq};
     R = BatchMPArray{g->r, g->lr, 1, g->lr};
+    tj.lock.unlock();
     return cudaSuccess;
 }
 
@@ -1193,10 +1274,29 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     const int prec = (int)(((long)(target * 3.322) + 31) / 32 + 1);
     Buf qbs, rbs;
     BatchMPArray Qbs, Rbs;
+    Buf p15b, q15b;
+    BatchMPArray P15, Q15;
+    bool have_sqrt = false;
     if (ckpt && ckpt_load(ckpt, N, qbs, Qbs, rbs, Rbs)) {
         *ckpt_state = 1;
     } else {
-        TRY(tree_run(ctx, pr, N, qbs, Qbs, rbs, Rbs, tuned));
+        TreeJoin tj;
+        TRY(tree_start(ctx, pr, N, qbs, Qbs, rbs, Rbs, tuned, tj));
+        if (tj.g && tuned) {
+            // the tree's graph runs on its own stream; sqrt(10005), which
+            // does not depend on it, runs meanwhile on this one (the same
+            // operations and integers, the side context's workspace)
+            BatchMPContext *side = side_context(ctx);
+            if (side) {
+                const cudaError_t e = sqrt_10005(side, pr, target, p15b, P15, q15b, Q15, tuned);
+                if (e != cudaSuccess) {
+                    tree_join(tj, qbs, Qbs, rbs, Rbs);
+                    return e;
+                }
+                have_sqrt = true;
+            }
+        }
+        TRY(tree_join(tj, qbs, Qbs, rbs, Rbs));
         if (ckpt) {
             // a file that cannot be written (unwritable directory, full
             // disk) does not fail the computation: state 3 reports it
@@ -1216,9 +1316,7 @@ static cudaError_t pi_fractional(BatchMPContext *ctx, Profiler *pr, int target, 
     long extra = std::max(0l, std::min((long)Qbs.length, (long)Rs.length) - prec);
     BatchMPArray Qt{Qbs.data + extra, Qbs.length - (uint32_t)extra, 1, Qbs.length - (uint32_t)extra};
     BatchMPArray Rt{Rs.data + extra, Rs.length - (uint32_t)extra, 1, Rs.length - (uint32_t)extra};
-    Buf p15b, q15b;
-    BatchMPArray P15, Q15;
-    TRY(sqrt_10005(ctx, pr, target, p15b, P15, q15b, Q15, tuned));
+    if (!have_sqrt) TRY(sqrt_10005(ctx, pr, target, p15b, P15, q15b, Q15, tuned));
     Buf pfb, qfb;
     BatchMPArray Pf{nullptr, P15.length + Qt.length, 1, P15.length + Qt.length};
     BatchMPArray Qf{nullptr, Q15.length + Rt.length, 1, Q15.length + Rt.length};
