@@ -68,12 +68,13 @@ NCU_TRAFFIC_SOURCE = {"ntt_rows_fused": "ncu capture of k_rows_r<12> on a 2^22 x
 # (profiles/int_pipes_pi1e8.md).  Scaled to this run's bytes and divided by
 # the live integer-pipe peaks they give each family's integer roofline.
 INT_WINST_PER_BYTE = {
-    "ntt_rows_level": (0.197852, 0.203125, 0.47631), "ntt_cols_fwd_first": (0.191449, 0.215956, 0.487502),
-    "ntt_cols_inv": (0.100019, 0.111781, 0.246528), "ntt_rows_fused": (0.223939, 0.221069, 0.529707),
-    "schoolbook_tc": (0.140841, 0.26468, 0.758519), "ntt_crt_carry": (0.075807, 0.089089, 0.220724),
-    "carry_chain": (0.078094, 0.116731, 0.274415), "schoolbook": (0.252166, 0.182724, 0.584128),
-    "ntt_cols_fwd": (0.078664, 0.093384, 0.199631), "ntt_local": (0.55531, 0.538007, 1.292256),
-    "ntt_coset_combine": (0.10361, 0.100811, 0.266338), "decimal_extract": (0.075693, 0.08626, 0.224201),
+    "ntt_rows_level": (0.20437, 0.205252, 0.487605), "ntt_cols_fwd_first": (0.187598, 0.211507, 0.477682),
+    "ntt_cols_inv": (0.100109, 0.11195, 0.246731), "schoolbook_tc": (0.143044, 0.265617, 0.763927),
+    "ntt_crt_carry": (0.075663, 0.095934, 0.230741), "ntt_rows_fused": (0.223057, 0.220512, 0.527792),
+    "schoolbook": (0.212093, 0.176371, 0.49994), "ntt_cols_fwd": (0.080255, 0.096138, 0.204625),
+    "carry_chain": (0.077046, 0.098004, 0.245578), "ntt_local": (0.55531, 0.538007, 1.292256),
+    "ntt_rows_inv": (0.078142, 0.077174, 0.193306), "ntt_rows_fwd": (0.10064, 0.094374, 0.250671),
+    "ntt_coset_combine": (0.103479, 0.100658, 0.265951), "decimal_extract": (0.075693, 0.08626, 0.224201),
     "decimal_leaf": (0.596097, 0.168555, 0.837855), "shift": (0.035647, 0.045182, 0.115069)}
 INT_SOURCE = ("ncu sm__inst_executed_pipe_{fmaheavy,alu}.sum and sm__inst_executed.sum over every launch of "
               "pi_bs_gpu 100000000 (profiles/int_pipes_pi1e8.md), per algorithmic byte, scaled to this run")

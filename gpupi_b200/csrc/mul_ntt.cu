@@ -377,12 +377,23 @@ __device__ __forceinline__ void rows_body(const NttParams &P, const RowsArgs &a,
         }
     }
     __syncthreads();
-    run_stages<LOG_C, 0, false, Q, 0>(xa, Sm, t, tw);
-    if (!a.square) {
-        // the tile is free again: every thread has passed the last stage's loads
-        // (A and B one after the other: a second tile would cost a CTA per SM)
-        __syncthreads();
-        run_stages<LOG_C, 0, false, Q, 0>(xb, Sm, t, tw);
+    // A then B through one copy of the forward stages (a loop, not two
+    // copies: smaller code for the instruction cache); B waits in xb and
+    // trades places with the transformed A between the passes.  A and B one
+    // after the other: a second tile would cost a CTA per SM.
+#pragma unroll 1
+    for (int op = 0; op < (a.square ? 1 : 2); ++op) {
+        if (op) {
+            // the tile is free again: every thread has passed the last stage's loads
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const uint32_t v = xa[j];
+                xa[j] = xb[j];
+                xb[j] = v;
+            }
+        }
+        run_stages<LOG_C, 0, false, Q, 0>(xa, Sm, t, tw);
     }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
@@ -660,42 +671,6 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
         for (uint32_t e = t; e < C - 1; e += T) tw[e] = __ldg(lev + e);
         __syncthreads();
     };
-    // kept operand F_keep; products F_keep F0 -> F0, F_keep F1 -> F1.  The
-    // first product waits in F0's own segment (word j of thread t at
-    // j * T + t, coalesced; every thread has loaded F0 before the stages'
-    // barriers, and reads back only its own words) while the second is
-    // formed: the segment is rewritten by the product's inverse anyway, and
-    // keeping it out of shared memory leaves room for a fourth CTA per SM.
-    // F0 null (uniform over the grid): the product F_keep F1 alone.
-    auto half = [&](const uint32_t *F_keep, uint32_t *F0, uint32_t *F1) {
-        uint32_t k[16], x[16];
-        table(levf);
-        load(F_keep, k);
-        run_stages<kSplitLogC, 0, false, Q, 0>(k, Sm, t, tw);
-        uint32_t *held = F0 ? F0 + off : nullptr;
-        if (held) {
-            __syncthreads();
-            load(F0, x);
-            run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) held[j * T + t] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
-        }
-        __syncthreads();
-        load(F1, x);
-        run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
-        table(levi);
-        run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
-        store(F1, x);
-        if (held) {
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < 16; ++j) x[j] = held[j * T + t];
-            run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
-            store(F0, x);
-        }
-    };
     // The six operand segments (16 KiB each, contiguous, 16-byte aligned) go
     // to L2 by bulk prefetch (the copy engine, no registers or shared memory)
     // as the CTA starts, so the later loads, issued between transforms, find
@@ -707,8 +682,55 @@ __device__ __forceinline__ void rows_level_body(const NttParams &P, const RowsLe
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F + off), "r"((uint32_t)C * 4u)
                          : "memory");
     }
-    half(a.Fpe, a.Fpo, a.Fro);
-    half(a.Fqo, a.Fqe, a.Fre);
+    // One copy of the forward and one of the inverse stages per prime, run
+    // in loops (the ten transforms written out would not fit the instruction
+    // cache).  Per half: the kept operand F_keep, then F0 (its product with
+    // F_keep waits in F0's own segment: word j of thread t at j * T + t,
+    // coalesced; every thread has loaded F0 before the next barrier and reads
+    // back only its own words; the segment is rewritten by the product's
+    // inverse anyway, and keeping the product out of shared memory leaves
+    // room for a fourth CTA per SM), then F1 (its product stays in registers);
+    // the inverse of F_keep F1 goes to F1, that of the held product to F0.
+    // F0 null (the tree's root, uniform over the grid): no P' product.
+    uint32_t k[16], x[16];
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t *Fk = h ? a.Fqo : a.Fpe;
+        uint32_t *F0 = h ? a.Fqe : a.Fpo;
+        uint32_t *F1 = h ? a.Fre : a.Fro;
+        uint32_t *held = F0 ? F0 + off : nullptr;
+        table(levf);
+#pragma unroll 1
+        for (int step = 0; step < 3; ++step) {
+            const uint32_t *src = step == 0 ? Fk : (step == 1 ? F0 : F1);
+            if (!src) continue;
+            if (step) __syncthreads();   // the previous transform has left the tile
+            load(src, x);
+            run_stages<kSplitLogC, 0, false, Q, 0>(x, Sm, t, tw);
+            if (step == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) k[j] = x[j];
+            } else if (step == 1) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) held[j * T + t] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) x[j] = norm<Q>(mont<Q>(mont<Q>(k[j], x[j]), scale));
+            }
+        }
+        table(levi);
+#pragma unroll 1
+        for (int step = 0; step < 2; ++step) {
+            if (step == 1) {
+                if (!held) break;
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) x[j] = held[j * T + t];
+            }
+            run_stages<kSplitLogC, 0, true, Q, 0>(x, Sm, t, tw);
+            store(step ? F0 : F1, x);
+        }
+    }
 }
 
 // the padded tile and the twiddle levels
