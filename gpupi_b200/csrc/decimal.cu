@@ -31,37 +31,63 @@ constexpr uint32_t kTen9 = 1000000000u;
 
 // out(pos) for the digit of place 10^-k (k = 1..L_dec):
 //   LSD-first layout (API): pos = L_dec - k;  natural layout: pos = k - 1.
+//
+// One thread per row; the CTA's 128 rows write their digits through shared
+// memory, eight 9-digit rounds (72 places) at a time: the CTA then stores
+// each row's 72-place run with consecutive threads on consecutive bytes,
+// instead of every thread storing single bytes one row apart (one sector
+// per lane per store).  The whole CTA runs every round (barriers); rows past
+// N compute nothing and store nothing.
+constexpr int kDecRows = 128;
+constexpr int kDecRounds = 8;
+constexpr int kDecSpan = 9 * kDecRounds;   // places per flush
+
 template <int MAXL, bool NATURAL>
-__global__ void __launch_bounds__(128) k_decimal_thread(const uint32_t *__restrict__ A,
-                                                        char *__restrict__ B, uint32_t N,
-                                                        uint32_t L, uint64_t sA, uint32_t L_dec,
-                                                        uint64_t sB) {
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < N;
-         row += gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(kDecRows) k_decimal_thread(const uint32_t *__restrict__ A,
+                                                             char *__restrict__ B, uint32_t N,
+                                                             uint32_t L, uint64_t sA, uint32_t L_dec,
+                                                             uint64_t sB) {
+    __shared__ char stage[kDecRows][kDecSpan + 1];
+    const uint32_t t = threadIdx.x;
+    for (uint64_t row0 = (uint64_t)blockIdx.x * kDecRows; row0 < N; row0 += (uint64_t)gridDim.x * kDecRows) {
+        const uint64_t row = row0 + t;
+        const bool valid = row < N;
+        const uint32_t rows = (N - row0 < (uint64_t)kDecRows) ? (uint32_t)(N - row0) : (uint32_t)kDecRows;
         uint32_t x[MAXL];
         const uint32_t *ar = A + row * sA;
         const uint32_t pad = MAXL - L;
 #pragma unroll
-        for (int i = 0; i < MAXL; ++i) x[i] = ((uint32_t)i >= pad) ? ar[i - pad] : 0u;
-        char *out = B + row * sB;
-        for (uint32_t start = 0; start < L_dec; start += 9u) {
-            uint32_t carry = 0u;
+        for (int i = 0; i < MAXL; ++i) x[i] = (valid && (uint32_t)i >= pad) ? ar[i - pad] : 0u;
+        for (uint32_t start = 0; start < L_dec; start += kDecSpan) {
+            const uint32_t span = min((uint32_t)kDecSpan, L_dec - start);
+            for (uint32_t r = 0; r * 9u < span; ++r) {
+                uint32_t carry = 0u;
 #pragma unroll
-            for (int i = 0; i < MAXL; ++i) {
-                const uint64_t t = (uint64_t)x[i] * kTen9 + carry;
-                x[i] = (uint32_t)t;
-                carry = (uint32_t)(t >> 32);
+                for (int i = 0; i < MAXL; ++i) {
+                    const uint64_t v = (uint64_t)x[i] * kTen9 + carry;
+                    x[i] = (uint32_t)v;
+                    carry = (uint32_t)(v >> 32);
+                }
+                // carry = the next 9 digits (places start + 9r + 1 .. + 9)
+                const uint32_t cnt = min(9u, span - r * 9u);
+                uint32_t v = carry;
+                for (uint32_t m = 9; m > cnt; --m) v /= 10u;   // drop places beyond L_dec
+                for (uint32_t m = cnt; m >= 1; --m) {
+                    stage[t][r * 9u + m - 1u] = (char)('0' + v % 10u);
+                    v /= 10u;
+                }
             }
-            // carry = next 9 digits (places start+1 .. start+9)
-            const uint32_t cnt = min(9u, L_dec - start);
-            uint32_t v = carry;
-            for (uint32_t m = 9; m > cnt; --m) v /= 10u;   // drop places beyond L_dec
-            for (uint32_t m = cnt; m >= 1; --m) {
-                const uint32_t k = start + m;   // place 10^-k
-                const char d = (char)('0' + v % 10u);
-                v /= 10u;
-                out[NATURAL ? (k - 1u) : (L_dec - k)] = d;
+            __syncthreads();
+            // places start + 1 .. start + span of rows row0 .. row0 + rows - 1;
+            // w / span as (w * ceil(2^32 / span)) >> 32, exact for w < 2^14
+            const uint64_t magic = (0x100000000ull + span - 1u) / span;
+            for (uint32_t w = t; w < rows * span; w += kDecRows) {
+                const uint32_t rr = (uint32_t)(((uint64_t)w * magic) >> 32);
+                const uint32_t j = w - rr * span;
+                const uint32_t k = start + j + 1u;   // place 10^-k
+                B[(row0 + rr) * sB + (NATURAL ? (k - 1u) : (L_dec - k))] = stage[rr][j];
             }
+            __syncthreads();
         }
     }
 }
