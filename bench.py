@@ -55,7 +55,7 @@ BBP_POSITIONS = 64
 # profiles/ntt_rows_level_pi1e8.md); applied to each launch of the family
 NCU_TRAFFIC_RATIO = {"ntt_rows_fused": 264.006 / 301.990,
                      "ntt_cols_fwd_first": 229.642496 / 234.881024,
-                     "ntt_rows_level": (2417.13 + 1586.67) / 4026.531840}
+                     "ntt_rows_level": (2630.51 + 1619.05) / 4026.531840}
 NCU_TRAFFIC_SOURCE = {"ntt_rows_fused": "ncu capture of k_rows_r<12> on a 2^22 x 2^22-limb product, "
                                         "scaled to each launch by its algorithmic bytes",
                       "ntt_cols_fwd_first": "ncu capture of k_cols_r<6, first, fwd, pair> on a 2^22 x 2^22-limb "
