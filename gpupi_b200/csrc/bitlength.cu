@@ -218,8 +218,8 @@ cudaError_t limb_length_prepare() { return length_state() ? cudaSuccess : cudaEr
 
 // The limb length of a batch written to device memory (d_out), without a
 // host synchronisation: the same scans, the result stored where one later
-// copy reads it.  Calls on the library's stream run in order, so the shared
-// max / ticket words are never used by two at once.
+// copy reads it.  Calls on one stream run in order and each stream has its
+// own max / ticket words, so a pair is never used by two scans at once.
 cudaError_t limb_length_to_device(const uint32_t *A, uint32_t N, uint32_t L, uint32_t stride, uint32_t *d_out) {
     LengthState *s = length_state();
     if (!s) return cudaErrorMemoryAllocation;
